@@ -1,0 +1,254 @@
+/*
+ * mtlgpu -- B200-native (sm_100a) sparse iterative-solve path for MTL4/ITL.
+ *
+ * C ABI.  Plain pointers and sizes only; no C++ or CUDA types cross this
+ * boundary (streams are passed as void*).  Every entry point returns an
+ * mtlgpu_status and never throws.  The header-only C++ layer
+ * <mtlgpu/mtl.hpp> maps these calls onto the MTL4/ITL names
+ * (mtl::compressed2D, itl::pc::ic_0, itl::cg, ...) and re-raises the
+ * reference's exception types.
+ *
+ * Each declaration cites the MTL4 interface it replaces (file:line inside the
+ * MTL4 tree).
+ *
+ * Conventions
+ *  - Matrices are CSR with int32 row pointers and column indices, rows sorted
+ *    by column, no duplicates (the invariant mtl::compressed2D keeps,
+ *    mtl/matrix/compressed2D.hpp:258-653).
+ *  - Vector arguments named d_* are DEVICE pointers of the context's device;
+ *    arguments named h_* are host pointers.  Device vectors are float64.
+ *  - All work of a context is ordered on the context's stream.  Calls on one
+ *    handle must be serialised by the caller; different contexts may be used
+ *    from different threads.  There is no hidden global state.
+ *  - A preconditioner handle keeps a non-owning reference to its matrix
+ *    handle: destroy the preconditioner first.
+ */
+#ifndef MTLGPU_H
+#define MTLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; only these entry points are
+ * exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define MTLGPU_ABI_VERSION 1
+
+/* Status codes.  MTLGPU_MAX_ITER has the value of basic_iteration's
+ * "Too many iterations" error code (itl/iteration/basic_iteration.hpp:43-48);
+ * the others map onto the reference's exceptions (mtl/utility/exception.hpp:
+ * 95-232, itl/utility/exception.hpp:22-31). */
+typedef enum {
+  MTLGPU_OK = 0,
+  MTLGPU_MAX_ITER = 1,          /* iteration limit reached */
+  MTLGPU_INVALID_ARG = 2,       /* null handle/pointer, negative size ...   */
+  MTLGPU_NOT_SQUARE = 3,        /* mtl::matrix_not_square                    */
+  MTLGPU_MISSING_DIAGONAL = 4,  /* mtl::missing_diagonal                     */
+  MTLGPU_ZERO_PIVOT = 5,        /* zero/non-positive/non-finite pivot; the
+                                   factors are still produced exactly as the
+                                   reference computes them (inf/NaN entries) */
+  MTLGPU_BREAKDOWN = 6,         /* itl::unexpected_orthogonality             */
+  MTLGPU_TIMEOUT = 7,           /* a bounded device wait ran out             */
+  MTLGPU_INTERRUPTED = 8,       /* the interrupt flag was raised             */
+  MTLGPU_CUDA_ERROR = 9,        /* CUDA runtime error (see mtlgpu_last_error) */
+  MTLGPU_NOT_SORTED = 10,       /* CSR rows not sorted / duplicate columns   */
+  MTLGPU_INDEX_RANGE = 11,      /* column index out of range                 */
+  MTLGPU_OUT_OF_MEMORY = 12,
+  MTLGPU_INCOMPATIBLE_SIZE = 13,/* mtl::incompatible_size                    */
+  MTLGPU_NOT_SUPPORTED = 14
+} mtlgpu_status;
+
+typedef enum { MTLGPU_FP64 = 0, MTLGPU_FP32 = 1 } mtlgpu_precision;
+
+/* itl/pc/identity.hpp:24-71, itl/pc/diagonal.hpp:28-103, itl/pc/ilu_0.hpp:86-92,
+ * itl/pc/ic_0.hpp:39-194 */
+typedef enum {
+  MTLGPU_PC_IDENTITY = 0,
+  MTLGPU_PC_DIAGONAL = 1,
+  MTLGPU_PC_ILU0 = 2,
+  MTLGPU_PC_IC0 = 3
+} mtlgpu_pc_kind;
+
+/* itl/krylov/cg.hpp:75-112, itl/krylov/bicgstab.hpp:27-78 */
+typedef enum { MTLGPU_CG = 0, MTLGPU_BICGSTAB = 1 } mtlgpu_method;
+
+/* Solve modes.
+ *  FP64         : the reference's arithmetic throughout (iteration counts
+ *                 track the reference's).
+ *  MIXED_REFINED: inner Krylov solve, factors and SpMV in FP32 (FP32 dots with
+ *                 compensated two-sum accumulation); FP64 outer iterative
+ *                 refinement r = b - A x, x += d and FP64 stopping norm.
+ *                 Requires a preconditioner created with factor precision
+ *                 MTLGPU_FP32. */
+typedef enum { MTLGPU_SOLVE_FP64 = 0, MTLGPU_SOLVE_MIXED_REFINED = 1 } mtlgpu_solve_mode;
+
+/* Which triangular factor (for sweeps and factor export). */
+typedef enum { MTLGPU_LOWER = 0, MTLGPU_UPPER = 1 } mtlgpu_factor;
+
+typedef struct mtlgpu_ctx mtlgpu_ctx;
+typedef struct mtlgpu_csr mtlgpu_csr;
+typedef struct mtlgpu_pc mtlgpu_pc;
+
+/* Iteration control: the fields of itl::basic_iteration(r0, max_iter, rtol,
+ * atol) (itl/iteration/basic_iteration.hpp:31-39): the solve stops when
+ * resid <= rtol * norm_r0 or resid <= atol (resid <= atol only when
+ * norm_r0 == 0); after max_iter iterations it stops with MTLGPU_MAX_ITER. */
+typedef struct {
+  int max_iter;
+  double rtol;
+  double atol;
+  double norm_r0;        /* < 0: use two_norm(b), as basic_iteration(b, ...) */
+  int mode;              /* mtlgpu_solve_mode */
+  /* MIXED_REFINED only: */
+  double inner_rtol;     /* relative reduction asked of each FP32 inner solve (0: 1e-4) */
+  int inner_max_iter;    /* per inner solve (0: max_iter)  */
+  int max_outer;         /* refinement steps (0: 30) */
+  /* optional: */
+  double* h_resid_history;   /* host array receiving every residual passed to
+                                the termination test, or NULL */
+  int history_cap;
+  const volatile int* h_interrupt; /* host flag (pinned or mapped memory is
+                                      best); nonzero stops the solve with
+                                      MTLGPU_INTERRUPTED between iterations,
+                                      as itl::interruptible_iteration */
+} mtlgpu_iter_params;
+
+typedef struct {
+  int error;             /* basic_iteration::error_code(): 0 or 1 (MAX_ITER) */
+  int status;            /* mtlgpu_status of the whole call */
+  int iterations;        /* basic_iteration::iterations() (total inner ones
+                            for MIXED_REFINED) */
+  int outer_iterations;  /* refinement steps (MIXED_REFINED), else 0 */
+  double resid;          /* last residual passed to the termination test */
+  double norm_r0;
+  double true_resid;     /* ||b - A x||_2 in FP64 at exit */
+  int history_len;       /* entries written to h_resid_history */
+} mtlgpu_iter_result;
+
+/* ---- context ----------------------------------------------------------- */
+mtlgpu_status mtlgpu_ctx_create(int device, mtlgpu_ctx** out);
+/* Use an existing stream (a cudaStream_t passed as void*). */
+mtlgpu_status mtlgpu_ctx_create_on_stream(int device, void* stream, mtlgpu_ctx** out);
+mtlgpu_status mtlgpu_ctx_destroy(mtlgpu_ctx* ctx);
+mtlgpu_status mtlgpu_ctx_synchronize(mtlgpu_ctx* ctx);
+void* mtlgpu_ctx_stream(mtlgpu_ctx* ctx);
+/* Upper bound on polls of one bounded device wait before it gives up with
+ * MTLGPU_TIMEOUT (default 1<<26). */
+mtlgpu_status mtlgpu_ctx_set_spin_limit(mtlgpu_ctx* ctx, long long polls);
+const char* mtlgpu_last_error(mtlgpu_ctx* ctx);
+const char* mtlgpu_status_string(int status);
+int mtlgpu_abi_version(void);
+
+/* Stream-ordered helpers for callers without a CUDA runtime of their own. */
+mtlgpu_status mtlgpu_malloc(mtlgpu_ctx* ctx, size_t bytes, void** d_out);
+mtlgpu_status mtlgpu_free(mtlgpu_ctx* ctx, void* d_ptr);
+mtlgpu_status mtlgpu_memcpy_h2d(mtlgpu_ctx* ctx, void* d_dst, const void* h_src, size_t bytes);
+mtlgpu_status mtlgpu_memcpy_d2h(mtlgpu_ctx* ctx, void* h_dst, const void* d_src, size_t bytes);
+
+/* ---- CSR matrix ---------------------------------------------------------
+ * Replaces compressed2D's raw-array constructor
+ * (mtl/matrix/compressed2D.hpp:355-364) and address_major/minor/data
+ * (610-620).  Arrays are copied in; the caller keeps ownership.  The pattern
+ * is validated on the device (sorted rows, indices in range). */
+mtlgpu_status mtlgpu_csr_create(mtlgpu_ctx* ctx, int n_rows, int n_cols, int nnz,
+                                const int32_t* h_row_ptr, const int32_t* h_col_idx,
+                                const double* h_vals, mtlgpu_csr** out);
+mtlgpu_status mtlgpu_csr_create_device(mtlgpu_ctx* ctx, int n_rows, int n_cols, int nnz,
+                                       const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                       const double* d_vals, mtlgpu_csr** out);
+/* New values on the same pattern (h_vals or d_vals, the other NULL). */
+mtlgpu_status mtlgpu_csr_set_values(mtlgpu_csr* A, const double* h_vals, const double* d_vals);
+mtlgpu_status mtlgpu_csr_destroy(mtlgpu_csr* A);
+/* num_rows, num_cols, nnz (compressed2D.hpp:636-640). */
+mtlgpu_status mtlgpu_csr_info(const mtlgpu_csr* A, int* n_rows, int* n_cols, int* nnz);
+/* Device views of the arrays (read-only for the caller). */
+mtlgpu_status mtlgpu_csr_device_arrays(const mtlgpu_csr* A, const int32_t** d_row_ptr,
+                                       const int32_t** d_col_idx, const double** d_vals);
+/* Choose SpMV row-bin thresholds by timing the candidates on this matrix
+ * (kept on the handle; reported in *h_choice when non-NULL). */
+mtlgpu_status mtlgpu_csr_autotune(mtlgpu_csr* A, int* h_choice);
+
+/* y = alpha * A * x + beta * y.  With (alpha, beta) = (1, 0), (1, 1), (-1, 1)
+ * this is y = A*x, y += A*x, y -= A*x (mtl/operation/mult.hpp:43-70,
+ * mtl/vector/crtp_base_vector.hpp:92-103,192-200,269-277, kernel
+ * mtl/operation/mat_vec_mult.hpp:620-689).  beta == 0 never reads y. */
+mtlgpu_status mtlgpu_spmv(mtlgpu_csr* A, const double* d_x, double* d_y, double alpha,
+                          double beta);
+/* y = A^T x (trans(A) * x; transposed_sparse_matrix_vector_product_test.cpp:32). */
+mtlgpu_status mtlgpu_spmv_transposed(mtlgpu_csr* A, const double* d_x, double* d_y);
+
+/* ---- BLAS-1 (mtl/operation/dot.hpp:226-232, two_norm.hpp:33-57,
+ *      unary_dot.hpp:29-65, vector/vec_vec_aop_expr.hpp:60-152).
+ *      Results are written to host scalars. */
+mtlgpu_status mtlgpu_dot(mtlgpu_ctx* ctx, int n, const double* d_x, const double* d_y,
+                         double* h_result);
+mtlgpu_status mtlgpu_two_norm(mtlgpu_ctx* ctx, int n, const double* d_x, double* h_result);
+mtlgpu_status mtlgpu_unary_dot(mtlgpu_ctx* ctx, int n, const double* d_x, double* h_result);
+/* y += alpha * x */
+mtlgpu_status mtlgpu_axpy(mtlgpu_ctx* ctx, int n, double alpha, const double* d_x, double* d_y);
+/* y = x + beta * y */
+mtlgpu_status mtlgpu_xpay(mtlgpu_ctx* ctx, int n, const double* d_x, double beta, double* d_y);
+
+/* ---- preconditioners ----------------------------------------------------
+ * Constructors itl::pc::identity<M>(A), diagonal<M>(A) (diagonal.hpp:37),
+ * ilu_0<M, V>(A) (ilu_0.hpp:92; factorisation ilu_0.hpp:45-82) and
+ * ic_0<M, V>(A) (ic_0.hpp:57; factorisation ic_0.hpp:136-186).  The
+ * factorisation always runs in FP64 on the device; factor_prec = MTLGPU_FP32
+ * stores the factors in FP32 as ilu_0<M, float> / ic_0<M, float> do
+ * (ic_0.hpp:122-130) and enables MIXED_REFINED solves.  The returned status
+ * reports MTLGPU_ZERO_PIVOT when a pivot is zero, negative (IC) or not finite;
+ * the handle is still created (the reference continues with inf/NaN). */
+mtlgpu_status mtlgpu_pc_create(mtlgpu_csr* A, int kind, int factor_prec, mtlgpu_pc** out);
+mtlgpu_status mtlgpu_pc_destroy(mtlgpu_pc* P);
+/* z = solve(P, r)  (ilu.hpp:84-91, ic_0.hpp:80-87, diagonal.hpp:57-64, pc/solver.hpp:23-52) */
+mtlgpu_status mtlgpu_pc_apply(mtlgpu_pc* P, const double* d_r, double* d_z);
+/* z = adjoint_solve(P, r) (ilu.hpp:106-115, ic_0.hpp:99-103, diagonal.hpp:75-82) */
+mtlgpu_status mtlgpu_pc_adjoint_apply(mtlgpu_pc* P, const double* d_r, double* d_z);
+/* One triangular sweep: MTLGPU_LOWER is lower_trisolve v5 (ILU, unit
+ * diagonal; lower_trisolve.hpp:173-189) or v6 (IC, inverted diagonal last;
+ * 192-209); MTLGPU_UPPER is upper_trisolve v3 (inverted diagonal first;
+ * upper_trisolve.hpp:160-176). */
+mtlgpu_status mtlgpu_pc_sweep(mtlgpu_pc* P, int which, const double* d_in, double* d_out);
+/* Factor sizes and level counts: nnz of the factor as the reference stores it
+ * (L of IC(0) includes the diagonal, L of ILU(0) does not). */
+mtlgpu_status mtlgpu_pc_factor_info(const mtlgpu_pc* P, int which, int* nnz, int* n_levels);
+/* Export a factor in the reference's CSR layout (get_L()/get_U(),
+ * ilu.hpp:118-119, ic_0.hpp:106-107) to host arrays of sizes n+1 / nnz / nnz.
+ * Values are exported as double (FP32 factors widened). */
+mtlgpu_status mtlgpu_pc_get_factor(const mtlgpu_pc* P, int which, int32_t* h_row_ptr,
+                                   int32_t* h_col_idx, double* h_vals);
+/* Level of every row in the factor's dependency graph (host array of n):
+ * level[r] = 0 for rows without off-diagonal entries, else 1 + max level of
+ * the off-diagonal columns (below the diagonal for LOWER, above it for
+ * UPPER). */
+mtlgpu_status mtlgpu_pc_get_levels(const mtlgpu_pc* P, int which, int32_t* h_levels);
+
+/* ---- solvers ------------------------------------------------------------
+ * itl::cg(A, x, b, P, iter) (cg.hpp:41-42,77-78) and
+ * itl::bicgstab(A, x, b, P, iter) (bicgstab.hpp:29-30).  x holds the initial
+ * guess on entry (warm start) and the solution on exit.  P may be NULL
+ * (identity).  The iteration state is returned in *res. */
+mtlgpu_status mtlgpu_solve(int method, mtlgpu_csr* A, mtlgpu_pc* P, double* d_x,
+                           const double* d_b, const mtlgpu_iter_params* params,
+                           mtlgpu_iter_result* res);
+/* Same with HOST x and b: copies b and x in, solves, copies x back. */
+mtlgpu_status mtlgpu_solve_host(int method, mtlgpu_csr* A, mtlgpu_pc* P, double* h_x,
+                                const double* h_b, const mtlgpu_iter_params* params,
+                                mtlgpu_iter_result* res);
+void mtlgpu_iter_params_default(mtlgpu_iter_params* p);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MTLGPU_H */

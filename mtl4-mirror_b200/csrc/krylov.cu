@@ -1,0 +1,843 @@
+// Device-resident CG and BiCGSTAB, captured into CUDA graphs.
+//
+// itl::cg (itl/krylov/cg.hpp:39-72 identity, 75-112 preconditioned) and
+// itl::bicgstab (itl/krylov/bicgstab.hpp:27-78), with basic_iteration control
+// (itl/iteration/basic_iteration.hpp:51-93).  All scalars (rho, alpha, ...)
+// live in a device SolverState; every kernel of an iteration reads what it
+// needs from there, reductions are deterministic grid reductions whose last
+// block also applies the reference's termination test, and every kernel
+// returns at once when the state says the solve has finished.  The host
+// launches a graph of kGraphIters iterations at a time and only looks at the
+// state between graph launches (that is also where the interrupt flag is
+// polled, as itl::interruptible_iteration does between iterations).
+//
+// Per CG iteration (preconditioned):
+//   sweeps   y0 = L^-1 r, z = U^-1 y0          (sweep.cu)
+//   K_rho    rho = r . z
+//   K_p      p = z (first) | z + (rho/rho_1) p
+//   K_spmv   q = A p, alpha_1 = p . q           (spmv.cu, fused epilogue)
+//   K_upd    alpha = rho/alpha_1, x += alpha p, r -= alpha q, rr = r . r,
+//            termination test on sqrt(|rr|); refills the sweep outputs with
+//            the sentinel for the next iteration.
+// The reference fuses q = A p with alpha_1 and r -= alpha q with rr in the
+// same way (fused_expr.hpp:57-77, cg.hpp:104,109).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace mtlgpu {
+
+using namespace dev;
+
+constexpr int kGraphIters = 8;
+
+struct SolverState {
+  int done;       // nonzero: every kernel returns immediately
+  int skip2;      // BiCGSTAB: second half of the iteration skipped
+  int half_exit;  // BiCGSTAB: finished on ||s||
+  int error;      // basic_iteration error code (0, 1)
+  int status;     // mtlgpu_status (BREAKDOWN, ...)
+  int iter;       // basic_iteration::i
+  int max_iter;
+  int hist_len;
+  int hist_cap;
+  int pad;
+  double tol;     // rtol * norm_r0
+  double atol;
+  double norm_r0;
+  double resid;
+  double rho, rho_1, rr, alpha_1, gamma, omega, ts, tt, ss;
+  double* history;
+};
+
+namespace {
+
+constexpr int kBlock = 256;
+
+int vec_grid(Ctx* ctx, long long n) {
+  long long need = (n + kBlock - 1) / kBlock;
+  long long cap = (long long)ctx->num_sms * 8;
+  return (int)std::max(1ll, std::min(need, cap));
+}
+
+// basic_iteration::finished(r) (basic_iteration.hpp:60-65 with converged()
+// 85-93 and check_max() 43-48).  Called by one thread.
+__device__ bool iter_finished(SolverState* st, double r) {
+  if (st->history && st->hist_len < st->hist_cap) st->history[st->hist_len] = r;
+  st->hist_len++;
+  st->resid = r;
+  bool conv = st->norm_r0 == 0.0 ? (r <= st->atol) : (r <= st->tol || r <= st->atol);
+  if (conv) return true;
+  if (st->iter >= st->max_iter) {
+    st->error = 1;
+    return true;
+  }
+  return false;
+}
+
+template <typename T>
+__device__ __forceinline__ typename AccOf<T, 1>::type acc1() {
+  return AccOf<T, 1>::type::zero();
+}
+
+// ---- generic pieces -----------------------------------------------------
+template <typename T>
+__global__ void fill2_kernel(int n, T* a, T* b) {
+  const T s = Box<T>::sentinel();
+  for (long long i = gtid(); i < n; i += gstride()) {
+    if (a) a[i] = s;
+    if (b) b[i] = s;
+  }
+}
+
+// first termination test after r = b - A x, rr = ||r||^2 (cg.hpp:93-95,
+// bicgstab.hpp:40-43)
+__global__ void init_check_kernel(SolverState* st, bool identity_pc) {
+  if (threadIdx.x != 0) return;
+  const double rr = st->rr;
+  if (identity_pc) st->rho = rr;  // unpreconditioned cg: rho = dot(r, r)
+  if (iter_finished(st, sqrt(fabs(rr)))) st->done = 1;
+}
+
+// rho = r . z
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    cg_rho_kernel(int n, const T* __restrict__ r, const T* __restrict__ z, SolverState* st,
+                  void* partials, unsigned* counter) {
+  if (st->done) return;
+  typedef typename AccOf<T, 1>::type R;
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) acc.add_prod(0, r[i], z[i]);
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) st->rho = tot.value(0);
+  }
+}
+
+// p = z (first iteration) | z + (rho / rho_1) p   (cg.hpp:99-102, 57-60)
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    cg_p_kernel(int n, const T* __restrict__ z, T* __restrict__ p, const SolverState* st) {
+  if (st->done) return;
+  if (st->iter == 0) {
+    for (long long i = gtid(); i < n; i += gstride()) p[i] = z[i];
+    return;
+  }
+  const T beta = (T)(st->rho / st->rho_1);
+  for (long long i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
+}
+
+// alpha = rho / alpha_1; x += alpha p; r -= alpha q; rr = r . r; next test.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    cg_update_kernel(int n, T* __restrict__ x, const T* __restrict__ p, T* __restrict__ r,
+                     const T* __restrict__ q, T* fill_a, T* fill_b, SolverState* st,
+                     bool identity_pc, void* partials, unsigned* counter) {
+  if (st->done) return;
+  typedef typename AccOf<T, 1>::type R;
+  const double alpha_d = st->rho / st->alpha_1;
+  const T alpha = (T)alpha_d;
+  const T s = Box<T>::sentinel();
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) {
+    x[i] += alpha * p[i];
+    const T ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    acc.add_prod(0, ri, ri);
+    if (fill_a) fill_a[i] = s;
+    if (fill_b) fill_b[i] = s;
+  }
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) {
+      const double rr = tot.value(0);
+      st->iter++;
+      st->rho_1 = st->rho;
+      st->rr = rr;
+      if (identity_pc) st->rho = rr;
+      if (iter_finished(st, sqrt(fabs(rr)))) st->done = 1;
+    }
+  }
+}
+
+// ---- BiCGSTAB -------------------------------------------------------------
+// rho_1 = rtilde . r, breakdown tests (bicgstab.hpp:45-52), ++iter.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    bicg_rho_kernel(int n, const T* __restrict__ rt, const T* __restrict__ r, SolverState* st,
+                    void* partials, unsigned* counter) {
+  if (st->done) return;
+  typedef typename AccOf<T, 1>::type R;
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) acc.add_prod(0, rt[i], r[i]);
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) {
+      st->iter++;
+      const double rho1 = tot.value(0);
+      st->rho = rho1;
+      if (rho1 == 0.0 || (st->iter > 1 && st->omega == 0.0)) {
+        st->status = MTLGPU_BREAKDOWN;
+        st->done = 1;
+        st->skip2 = 1;
+      }
+    }
+  }
+}
+
+// p = r (first) | r + beta (p - omega v), beta = (rho_1/rho_2)(alpha/omega)
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    bicg_p_kernel(int n, const T* __restrict__ r, T* __restrict__ p, const T* __restrict__ v,
+                  const SolverState* st) {
+  if (st->done) return;
+  if (st->iter <= 1) {
+    for (long long i = gtid(); i < n; i += gstride()) p[i] = r[i];
+    return;
+  }
+  // st->rho_1 holds rho_2 (previous rho), st->alpha_1 the previous alpha
+  const double beta_d = (st->rho / st->rho_1) * (st->alpha_1 / st->omega);
+  const T beta = (T)beta_d, omega = (T)st->omega;
+  for (long long i = gtid(); i < n; i += gstride()) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+}
+
+// alpha = rho_1 / gamma; s = r - alpha v; ||s||; half-step termination test
+// (bicgstab.hpp:58-67).
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    bicg_s_kernel(int n, const T* __restrict__ r, const T* __restrict__ v, T* __restrict__ s,
+                  T* fill_a, T* fill_b, SolverState* st, void* partials, unsigned* counter) {
+  if (st->done) return;
+  typedef typename AccOf<T, 1>::type R;
+  const double gamma = st->gamma;
+  const T alpha = (T)(st->rho / gamma);
+  const T sent = Box<T>::sentinel();
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) {
+    const T si = r[i] - alpha * v[i];
+    s[i] = si;
+    acc.add_prod(0, si, si);
+    if (fill_a) fill_a[i] = sent;
+    if (fill_b) fill_b[i] = sent;
+  }
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) {
+      if (gamma == 0.0) {
+        st->status = MTLGPU_BREAKDOWN;
+        st->done = 1;
+        st->skip2 = 1;
+      } else {
+        st->alpha_1 = st->rho / gamma;  // alpha
+        st->ss = tot.value(0);
+        if (iter_finished(st, sqrt(st->ss))) {
+          st->half_exit = 1;
+          st->skip2 = 1;
+        }
+      }
+    }
+  }
+}
+
+// x += omega shat + alpha phat, r = s - omega t, ||r|| and the loop test
+// (bicgstab.hpp:70-75, 43); on a half-step exit only x += alpha phat.
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    bicg_x_kernel(int n, T* __restrict__ x, const T* __restrict__ phat, const T* __restrict__ shat,
+                  const T* __restrict__ s, const T* __restrict__ t, T* __restrict__ r, T* fill_a,
+                  T* fill_b, SolverState* st, void* partials, unsigned* counter) {
+  if (st->done) return;
+  typedef typename AccOf<T, 1>::type R;
+  const T alpha = (T)st->alpha_1;
+  if (st->half_exit) {
+    for (long long i = gtid(); i < n; i += gstride()) x[i] += alpha * phat[i];
+    __syncthreads();
+    if (publish_partial(R::zero(), reinterpret_cast<R*>(partials), blockIdx.x, counter,
+                        gridDim.x)) {
+      if (threadIdx.x == 0) st->done = 1;
+    }
+    return;
+  }
+  const double omega_d = st->ts / st->tt;
+  const T omega = (T)omega_d;
+  const T sent = Box<T>::sentinel();
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) {
+    x[i] += omega * shat[i] + alpha * phat[i];
+    const T ri = s[i] - omega * t[i];
+    r[i] = ri;
+    acc.add_prod(0, ri, ri);
+    if (fill_a) fill_a[i] = sent;
+    if (fill_b) fill_b[i] = sent;
+  }
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) {
+      st->omega = omega_d;
+      st->rho_1 = st->rho;  // rho_2 = rho_1
+      const double rr = tot.value(0);
+      st->rr = rr;
+      if (iter_finished(st, sqrt(rr))) st->done = 1;
+    }
+  }
+}
+
+// t . s and t . t after t = A shat (omega = dot(t,s) / dot(t,t)).
+template <typename T>
+__global__ void __launch_bounds__(kBlock)
+    bicg_omega_kernel(int n, const T* __restrict__ t, const T* __restrict__ s, SolverState* st,
+                      void* partials, unsigned* counter) {
+  if (st->done || st->skip2) return;
+  typedef typename AccOf<T, 2>::type R;
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) {
+    acc.add_prod(0, t[i], s[i]);
+    acc.add_prod(1, t[i], t[i]);
+  }
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) {
+      st->ts = tot.value(0);
+      st->tt = tot.value(1);
+    }
+  }
+}
+
+// The second half of an iteration runs unless the solve is over.
+__global__ void bicg_reset_skip_kernel(SolverState* st) {
+  if (threadIdx.x == 0) st->skip2 = st->done ? 1 : 0;
+}
+
+// ---- mixed precision helpers ----------------------------------------------
+__global__ void scale_to_f32_kernel(int n, const double* __restrict__ r, double inv_scale,
+                                    float* __restrict__ r32, float* __restrict__ x32) {
+  for (long long i = gtid(); i < n; i += gstride()) {
+    r32[i] = (float)(r[i] * inv_scale);
+    x32[i] = 0.f;
+  }
+}
+__global__ void refine_update_kernel(int n, double* __restrict__ x, const float* __restrict__ d,
+                                     double scale) {
+  for (long long i = gtid(); i < n; i += gstride()) x[i] += scale * (double)d[i];
+}
+
+// Inner FP32 solve starting from x = 0: r = rhs, rr = ||r||^2.
+__global__ void __launch_bounds__(kBlock)
+    f32_norm_kernel(int n, const float* __restrict__ r, SolverState* st, void* partials,
+                    unsigned* counter) {
+  typedef CSum<1> R;
+  R acc = R::zero();
+  for (long long i = gtid(); i < n; i += gstride()) acc.add_prod(0, r[i], r[i]);
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) st->rr = tot.value(0);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Workspace: buffers, device state and the instantiated graph of one
+// (matrix, preconditioner, method, precision) combination.
+template <typename T>
+struct Workspace {
+  Csr* A = nullptr;
+  Pc* P = nullptr;
+  int method = MTLGPU_CG;
+  int n = 0;
+  T *x = nullptr, *b = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr,
+    *rt = nullptr, *phat = nullptr, *s = nullptr, *shat = nullptr, *t = nullptr, *v = nullptr;
+  SolverState* st = nullptr;   // device
+  SolverState* h_st = nullptr; // pinned host mirror
+  double* history = nullptr;
+  int hist_cap = 0;
+  cudaGraphExec_t exec = nullptr;
+  ~Workspace() {}
+};
+
+namespace {
+
+bool is_identity(Pc* P) { return !P || P->kind == MTLGPU_PC_IDENTITY; }
+
+template <typename T>
+T* pc_tmp(Pc* P);
+template <>
+double* pc_tmp<double>(Pc* P) { return P ? P->d_tmp : nullptr; }
+template <>
+float* pc_tmp<float>(Pc* P) { return P ? P->d_tmp32 : nullptr; }
+
+bool uses_sweeps(Pc* P) { return P && (P->kind == MTLGPU_PC_IC0 || P->kind == MTLGPU_PC_ILU0); }
+
+template <typename T>
+__global__ void copy_if_kernel(int n, const T* __restrict__ a, T* __restrict__ b, const int* skip) {
+  if (*skip) return;
+  for (long long i = gtid(); i < n; i += gstride()) b[i] = a[i];
+}
+
+// z = solve(P, r); a missing preconditioner is the identity.
+template <typename T>
+mtlgpu_status apply_pc(Workspace<T>* W, const T* r, T* z, const int* skip, bool prefilled) {
+  if (W->P) return pc_apply_t<T>(W->P, r, z, false, skip, prefilled, prefilled);
+  Ctx* ctx = W->A->ctx;
+  copy_if_kernel<T><<<vec_grid(ctx, W->n), kBlock, 0, ctx->stream>>>(W->n, r, z, skip);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+// Kernels of one CG iteration.
+template <typename T>
+mtlgpu_status record_cg_iteration(Workspace<T>* W) {
+  Csr* A = W->A;
+  Ctx* ctx = A->ctx;
+  const int n = W->n;
+  const int grid = vec_grid(ctx, n);
+  const bool ident = is_identity(W->P);
+  const int* skip = &W->st->done;
+  T* zvec = W->r;
+  if (!ident) {
+    zvec = W->z;
+    const bool sw = uses_sweeps(W->P);
+    MTLGPU_TRY(pc_apply_t<T>(W->P, W->r, W->z, false, skip, sw, sw));
+    cg_rho_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->z, W->st, ctx->d_partials,
+                                                       counter_slot(ctx, 1));
+  }
+  cg_p_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, zvec, W->p, W->st);
+  SpmvArgs a;
+  a.epi = EPI_DOT_X2;
+  a.x2 = W->p;
+  a.out = &W->st->alpha_1;
+  a.skip = skip;
+  MTLGPU_TRY(spmv_launch<T>(A, W->p, W->q, a));
+  T* fa = uses_sweeps(W->P) ? pc_tmp<T>(W->P) : nullptr;
+  T* fb = uses_sweeps(W->P) ? W->z : nullptr;
+  cg_update_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->x, W->p, W->r, W->q, fa, fb, W->st,
+                                                        ident, ctx->d_partials,
+                                                        counter_slot(ctx, 2));
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+// Kernels of one BiCGSTAB iteration.
+template <typename T>
+mtlgpu_status record_bicgstab_iteration(Workspace<T>* W) {
+  Csr* A = W->A;
+  Ctx* ctx = A->ctx;
+  const int n = W->n;
+  const int grid = vec_grid(ctx, n);
+  const bool sw = uses_sweeps(W->P);
+  T* tmp = pc_tmp<T>(W->P);
+  bicg_reset_skip_kernel<<<1, 32, 0, ctx->stream>>>(W->st);
+  bicg_rho_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->rt, W->r, W->st, ctx->d_partials,
+                                                       counter_slot(ctx, 3));
+  bicg_p_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->p, W->v, W->st);
+  // phat = solve(M, p)  (sweep outputs prefilled by the previous x-update)
+  MTLGPU_TRY(apply_pc<T>(W, W->p, W->phat, &W->st->done, sw));
+  SpmvArgs a;
+  a.epi = EPI_DOT_X2;
+  a.x2 = W->rt;
+  a.out = &W->st->gamma;
+  a.skip = &W->st->done;
+  MTLGPU_TRY(spmv_launch<T>(A, W->phat, W->v, a));
+  bicg_s_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->v, W->s, sw ? tmp : nullptr,
+                                                     sw ? W->shat : nullptr, W->st,
+                                                     ctx->d_partials, counter_slot(ctx, 4));
+  // shat = solve(M, s); t = A shat; omega
+  MTLGPU_TRY(apply_pc<T>(W, W->s, W->shat, &W->st->skip2, sw));
+  SpmvArgs a2;
+  a2.epi = EPI_AXPBY;
+  a2.skip = &W->st->skip2;
+  MTLGPU_TRY(spmv_launch<T>(A, W->shat, W->t, a2));
+  bicg_omega_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->t, W->s, W->st, ctx->d_partials,
+                                                         counter_slot(ctx, 5));
+  bicg_x_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->x, W->phat, W->shat, W->s, W->t, W->r,
+                                                     sw ? tmp : nullptr, sw ? W->phat : nullptr,
+                                                     W->st, ctx->d_partials, counter_slot(ctx, 6));
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+template <typename T>
+mtlgpu_status build_graph(Workspace<T>* W) {
+  Ctx* ctx = W->A->ctx;
+  if (W->exec) return MTLGPU_OK;
+  cudaGraph_t g = nullptr;
+  MTLGPU_TRY_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  mtlgpu_status s = MTLGPU_OK;
+  for (int k = 0; k < kGraphIters && s == MTLGPU_OK; k++)
+    s = W->method == MTLGPU_CG ? record_cg_iteration<T>(W) : record_bicgstab_iteration<T>(W);
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (s != MTLGPU_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  MTLGPU_TRY_CUDA(ctx, e);
+  e = cudaGraphInstantiate(&W->exec, g, 0);
+  cudaGraphDestroy(g);
+  MTLGPU_TRY_CUDA(ctx, e);
+  return MTLGPU_OK;
+}
+
+template <typename T>
+mtlgpu_status alloc_workspace(Workspace<T>* W) {
+  Ctx* ctx = W->A->ctx;
+  const int n = W->n;
+  MTLGPU_TRY(dalloc(ctx, &W->x, n));
+  MTLGPU_TRY(dalloc(ctx, &W->b, n));
+  MTLGPU_TRY(dalloc(ctx, &W->r, n));
+  MTLGPU_TRY(dalloc(ctx, &W->p, n));
+  MTLGPU_TRY(dalloc(ctx, &W->q, n));
+  if (!is_identity(W->P) || W->method == MTLGPU_BICGSTAB) MTLGPU_TRY(dalloc(ctx, &W->z, n));
+  if (W->method == MTLGPU_BICGSTAB) {
+    MTLGPU_TRY(dalloc(ctx, &W->rt, n));
+    MTLGPU_TRY(dalloc(ctx, &W->phat, n));
+    MTLGPU_TRY(dalloc(ctx, &W->s, n));
+    MTLGPU_TRY(dalloc(ctx, &W->shat, n));
+    MTLGPU_TRY(dalloc(ctx, &W->t, n));
+    MTLGPU_TRY(dalloc(ctx, &W->v, n));
+    MTLGPU_TRY_CUDA(ctx, cudaMemsetAsync(W->v, 0, sizeof(T) * n, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaMemsetAsync(W->p, 0, sizeof(T) * n, ctx->stream));
+  }
+  MTLGPU_TRY(dalloc(ctx, &W->st, 1));
+  MTLGPU_TRY_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&W->h_st), sizeof(SolverState)));
+  return MTLGPU_OK;
+}
+
+template <typename T>
+void release_workspace(Workspace<T>* W) {
+  if (!W) return;
+  Ctx* ctx = W->A->ctx;
+  if (W->exec) cudaGraphExecDestroy(W->exec);
+  T** bufs[] = {&W->x, &W->b, &W->r, &W->z, &W->p, &W->q, &W->rt, &W->phat, &W->s, &W->shat,
+                &W->t, &W->v};
+  for (T** b : bufs) dfree(ctx, *b);
+  dfree(ctx, W->st);
+  dfree(ctx, W->history);
+  if (W->h_st) cudaFreeHost(W->h_st);
+  W->h_st = nullptr;
+}
+
+}  // namespace
+
+// Releases every workspace of A (called when A or a preconditioner of A is destroyed).
+void release_workspaces(Csr* A, Pc* only_P);
+
+namespace {
+
+constexpr int prec_of(double*) { return MTLGPU_FP64; }
+constexpr int prec_of(float*) { return MTLGPU_FP32; }
+
+// Workspaces are cached on the matrix handle, keyed by (preconditioner,
+// method, precision); nothing is shared between handles.
+template <typename T>
+mtlgpu_status get_workspace(Csr* A, Pc* P, int method, Workspace<T>** out) {
+  const int prec = prec_of((T*)nullptr);
+  for (auto& e : A->workspaces)
+    if (e.P == P && e.method == method && e.prec == prec) {
+      *out = static_cast<Workspace<T>*>(e.ws);
+      return MTLGPU_OK;
+    }
+  Workspace<T>* W = new Workspace<T>();
+  W->A = A;
+  W->P = P;
+  W->method = method;
+  W->n = A->n_rows;
+  mtlgpu_status s = alloc_workspace<T>(W);
+  if (s != MTLGPU_OK) {
+    release_workspace<T>(W);
+    delete W;
+    return s;
+  }
+  A->workspaces.push_back({P, method, prec, W});
+  *out = W;
+  return MTLGPU_OK;
+}
+
+template <typename T>
+mtlgpu_status ensure_history(Workspace<T>* W, int cap) {
+  if (cap <= W->hist_cap) return MTLGPU_OK;
+  Ctx* ctx = W->A->ctx;
+  dfree(ctx, W->history);
+  MTLGPU_TRY(dalloc(ctx, &W->history, cap));
+  W->hist_cap = cap;
+  if (W->exec) {  // state pointer unchanged; the history pointer lives in the state
+  }
+  return MTLGPU_OK;
+}
+
+// Runs graph launches until the state reports completion.
+template <typename T>
+mtlgpu_status run_iterations(Workspace<T>* W, const volatile int* h_interrupt, int* interrupted) {
+  Ctx* ctx = W->A->ctx;
+  MTLGPU_TRY(build_graph<T>(W));
+  *interrupted = 0;
+  while (true) {
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->h_st, W->st, sizeof(SolverState),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (W->h_st->done) break;
+    if (h_interrupt && *h_interrupt) {
+      *interrupted = 1;
+      break;
+    }
+    int err = 0;
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaGraphLaunch(W->exec, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (err) break;
+  }
+  return take_device_error(ctx);
+}
+
+template <typename T>
+void init_state(SolverState* h, const mtlgpu_iter_params* prm, double norm_r0, int max_iter,
+                double* history, int hist_cap) {
+  std::memset(h, 0, sizeof(SolverState));
+  h->max_iter = max_iter;
+  h->tol = prm->rtol * norm_r0;
+  h->atol = prm->atol;
+  h->norm_r0 = norm_r0;
+  h->history = history;
+  h->hist_cap = hist_cap;
+}
+
+// One complete device solve in precision T on workspace W (x, b already in
+// W->x, W->b; or, with rhs_is_residual, W->r holds the rhs and x = 0).
+template <typename T>
+mtlgpu_status device_solve(Workspace<T>* W, const mtlgpu_iter_params* prm, double norm_r0,
+                           bool norm_from_b, int max_iter, bool rhs_is_residual, int* iters,
+                           int* err_code, int* status, double* resid, int* hist_len,
+                           double* h_hist, int h_hist_cap) {
+  Csr* A = W->A;
+  Ctx* ctx = A->ctx;
+  const int n = W->n;
+  const int cap = std::max(2 * max_iter + 4, 16);
+  MTLGPU_TRY(ensure_history<T>(W, cap));
+  const bool ident = is_identity(W->P);
+  const bool sw = uses_sweeps(W->P);
+  // norm_r0 = two_norm(b) when asked (basic_iteration(b, ...))
+  if (norm_from_b) {
+    SpmvArgs dummy;
+    (void)dummy;
+    MTLGPU_TRY(dot_launch(ctx, n, reinterpret_cast<const double*>(W->b),
+                          reinterpret_cast<const double*>(W->b), ctx->d_scalars, 1));
+    double nb2 = 0;
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&nb2, ctx->d_scalars, sizeof(double),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    norm_r0 = std::sqrt(nb2);
+  }
+  init_state<T>(W->h_st, prm, norm_r0, max_iter, W->history, W->hist_cap);
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->st, W->h_st, sizeof(SolverState), cudaMemcpyHostToDevice,
+                                       ctx->stream));
+  const int grid = vec_grid(ctx, n);
+  if (rhs_is_residual) {
+    f32_norm_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, reinterpret_cast<const float*>(W->r),
+                                                      W->st, ctx->d_partials,
+                                                      counter_slot(ctx, 7));
+  } else {
+    SpmvArgs a;
+    a.epi = EPI_RESID;
+    a.b = W->b;
+    a.out = &W->st->rr;
+    MTLGPU_TRY(spmv_launch<T>(A, W->x, W->r, a));  // r = b - A x, rr
+  }
+  if (W->method == MTLGPU_BICGSTAB)
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->rt, W->r, sizeof(T) * n, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+  init_check_kernel<<<1, 32, 0, ctx->stream>>>(W->st, ident && W->method == MTLGPU_CG);
+  if (sw) {
+    T* second = W->method == MTLGPU_CG ? W->z : W->phat;
+    fill2_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, pc_tmp<T>(W->P), second);
+  }
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  int interrupted = 0;
+  MTLGPU_TRY(run_iterations<T>(W, prm->h_interrupt, &interrupted));
+  SolverState* h = W->h_st;
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h, W->st, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+  MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *iters = h->iter;
+  *err_code = h->error;
+  *status = interrupted ? MTLGPU_INTERRUPTED : (h->status ? h->status : (h->error ? MTLGPU_MAX_ITER : MTLGPU_OK));
+  *resid = h->resid;
+  *hist_len = h->hist_len;
+  if (h_hist && h_hist_cap > 0) {
+    int m = std::min(std::min(h->hist_len, W->hist_cap), h_hist_cap);
+    if (m > 0) {
+      MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h_hist, W->history, sizeof(double) * m,
+                                           cudaMemcpyDeviceToHost, ctx->stream));
+      MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+  }
+  return MTLGPU_OK;
+}
+
+mtlgpu_status true_residual(Csr* A, const double* x, const double* b, double* scratch,
+                            double* out) {
+  Ctx* ctx = A->ctx;
+  SpmvArgs a;
+  a.epi = EPI_RESID;
+  a.b = b;
+  a.out = ctx->d_scalars + 2;
+  MTLGPU_TRY(spmv_launch<double>(A, x, scratch, a));
+  double rr = 0;
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&rr, ctx->d_scalars + 2, sizeof(double),
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+  MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *out = std::sqrt(rr);
+  return MTLGPU_OK;
+}
+
+}  // namespace
+
+void release_workspaces(Csr* A, Pc* only_P) {
+  std::vector<WorkspaceEntry> keep;
+  for (auto& e : A->workspaces) {
+    if (only_P && e.P != only_P) {
+      keep.push_back(e);
+      continue;
+    }
+    if (e.prec == MTLGPU_FP64) {
+      auto* W = static_cast<Workspace<double>*>(e.ws);
+      release_workspace<double>(W);
+      delete W;
+    } else {
+      auto* W = static_cast<Workspace<float>*>(e.ws);
+      release_workspace<float>(W);
+      delete W;
+    }
+  }
+  A->workspaces = keep;
+}
+
+// Iterative refinement: FP32 inner solves, FP64 residual / update / norm.
+static mtlgpu_status solve_mixed(int method, Csr* A, Pc* P, double* d_x, const double* d_b,
+                                 const mtlgpu_iter_params* prm, mtlgpu_iter_result* res) {
+  Ctx* ctx = A->ctx;
+  const int n = A->n_rows;
+  if (P && P->prec != MTLGPU_FP32 && P->kind != MTLGPU_PC_IDENTITY) return MTLGPU_INVALID_ARG;
+  MTLGPU_TRY(csr_ensure_fp32(A));
+  Workspace<double>* W64 = nullptr;
+  Workspace<float>* W32 = nullptr;
+  MTLGPU_TRY(get_workspace<double>(A, P, -1 - method, &W64));  // buffers only
+  MTLGPU_TRY(get_workspace<float>(A, P, method, &W32));
+  const int grid = vec_grid(ctx, n);
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W64->x, d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+  double norm_r0 = prm->norm_r0;
+  if (norm_r0 < 0) {
+    MTLGPU_TRY(dot_launch(ctx, n, d_b, d_b, ctx->d_scalars, 1));
+    double nb2 = 0;
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&nb2, ctx->d_scalars, sizeof(double),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    norm_r0 = std::sqrt(nb2);
+  }
+  const double tol = prm->rtol * norm_r0;
+  const double inner_rtol = prm->inner_rtol > 0 ? prm->inner_rtol : 1e-4;
+  const int max_outer = prm->max_outer > 0 ? prm->max_outer : 30;
+  const int inner_max = prm->inner_max_iter > 0 ? prm->inner_max_iter : prm->max_iter;
+  int total = 0, outer = 0, hist = 0;
+  res->status = MTLGPU_OK;
+  res->error = 0;
+  double resid = 0;
+  while (true) {
+    MTLGPU_TRY(true_residual(A, W64->x, d_b, W64->r, &resid));
+    if (prm->h_resid_history && hist < prm->history_cap) prm->h_resid_history[hist] = resid;
+    hist++;
+    const bool conv = norm_r0 == 0 ? resid <= prm->atol : (resid <= tol || resid <= prm->atol);
+    if (conv) break;
+    if (outer >= max_outer || total >= prm->max_iter) {
+      res->error = 1;
+      res->status = MTLGPU_MAX_ITER;
+      break;
+    }
+    if (prm->h_interrupt && *prm->h_interrupt) {
+      res->status = MTLGPU_INTERRUPTED;
+      break;
+    }
+    // inner: A d = r / ||r|| in FP32 from d = 0
+    scale_to_f32_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, W64->r, 1.0 / resid, W32->r, W32->x);
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    mtlgpu_iter_params ip = *prm;
+    ip.rtol = inner_rtol;
+    ip.atol = 0;
+    int it = 0, ec = 0, st = 0, hl = 0;
+    double rr = 0;
+    MTLGPU_TRY(device_solve<float>(W32, &ip, 1.0, false, std::min(inner_max, prm->max_iter - total),
+                                   true, &it, &ec, &st, &rr, &hl, nullptr, 0));
+    total += it;
+    outer++;
+    if (st == MTLGPU_BREAKDOWN || st == MTLGPU_TIMEOUT || st == MTLGPU_INTERRUPTED) {
+      res->status = st;
+      if (st != MTLGPU_BREAKDOWN) break;
+    }
+    refine_update_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, W64->x, W32->x, resid);
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    if (st == MTLGPU_BREAKDOWN) break;
+  }
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(d_x, W64->x, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+  res->iterations = total;
+  res->outer_iterations = outer;
+  res->resid = resid;
+  res->norm_r0 = norm_r0;
+  res->true_resid = resid;
+  res->history_len = hist;
+  MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return (mtlgpu_status)res->status;
+}
+
+mtlgpu_status solve_impl(int method, Csr* A, Pc* P, double* d_x, const double* d_b,
+                         const mtlgpu_iter_params* prm, mtlgpu_iter_result* res) {
+  Ctx* ctx = A->ctx;
+  std::memset(res, 0, sizeof(*res));
+  if (A->n_rows != A->n_cols) return MTLGPU_NOT_SQUARE;
+  if (P && P->A != A) return MTLGPU_INVALID_ARG;
+  if (method != MTLGPU_CG && method != MTLGPU_BICGSTAB) return MTLGPU_INVALID_ARG;
+  if (prm->mode == MTLGPU_SOLVE_MIXED_REFINED) return solve_mixed(method, A, P, d_x, d_b, prm, res);
+  const int n = A->n_rows;
+  Workspace<double>* W = nullptr;
+  MTLGPU_TRY(get_workspace<double>(A, P, method, &W));
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->x, d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->b, d_b, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+  int it = 0, ec = 0, st = 0, hl = 0;
+  double resid = 0;
+  MTLGPU_TRY(device_solve<double>(W, prm, prm->norm_r0, prm->norm_r0 < 0, prm->max_iter, false, &it,
+                                  &ec, &st, &resid, &hl, prm->h_resid_history, prm->history_cap));
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(d_x, W->x, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+  res->iterations = it;
+  res->error = ec;
+  res->status = st;
+  res->resid = resid;
+  res->norm_r0 = W->h_st->norm_r0;
+  res->history_len = hl;
+  double tr = 0;
+  MTLGPU_TRY(true_residual(A, W->x, W->b, W->q, &tr));
+  res->true_resid = tr;
+  return (mtlgpu_status)st;
+}
+
+}  // namespace mtlgpu

@@ -1,0 +1,389 @@
+// CSR sparse matrix-vector products for sm_100a.
+//
+// Replaces smat_cvec_mult<compressed2D> (mtl/operation/mat_vec_mult.hpp:
+// 620-689) and the fused row evaluator of CG (mtl/vector/
+// row_mat_cvec_index_evaluator.hpp:26-67 with dot_index_evaluator.hpp:19-45).
+//
+// Design: rows are binned by length; a bin with G lanes per row runs
+// spmv_group<G>: each G-lane group walks its row with stride G (coalesced
+// loads of values and column indices across the warp), gathers x through the
+// read-only path (x stays resident in the 126 MB L2 for every configuration
+// here), reduces with shuffles and lane 0 writes the row result and feeds
+// the optional epilogue reduction.  Rows longer than 1024 entries get a CTA
+// each.  Grids are persistent-style (a multiple of the SM count) so that
+// epilogue reductions have a fixed number of partials and are deterministic.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace mtlgpu {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ int pow2_group(int len) {
+  int g = 2;
+  while (g < len && g < 32) g <<= 1;
+  return g;
+}
+
+// Row statistics, validation and diagonal positions.
+__global__ void csr_analyse_kernel(int n_rows, int n_cols, int nnz, const int32_t* __restrict__ rp,
+                                   const int32_t* __restrict__ ci, int32_t* __restrict__ diag,
+                                   unsigned long long* stats, int* err) {
+  // stats[0] = max row length, stats[1] = sum of row lengths
+  unsigned long long my_max = 0, my_sum = 0;
+  for (long long r = gtid(); r < n_rows; r += gstride()) {
+    int b = rp[r], e = rp[r + 1];
+    if (r == 0 && b != 0) atomicCAS(err, 0, (int)MTLGPU_INVALID_ARG);
+    if (r == n_rows - 1 && e != nnz) atomicCAS(err, 0, (int)MTLGPU_INVALID_ARG);
+    if (e < b || b < 0 || e > nnz) {
+      atomicCAS(err, 0, (int)MTLGPU_INVALID_ARG);
+      diag[r] = -1;
+      continue;
+    }
+    int d = -1, prev = -1;
+    for (int j = b; j < e; j++) {
+      int c = ci[j];
+      if (c < 0 || c >= n_cols) atomicCAS(err, 0, (int)MTLGPU_INDEX_RANGE);
+      if (c <= prev) atomicCAS(err, 0, (int)MTLGPU_NOT_SORTED);
+      if (c == r) d = j;
+      prev = c;
+    }
+    diag[r] = d;
+    unsigned long long len = (unsigned long long)(e - b);
+    my_max = len > my_max ? len : my_max;
+    my_sum += len;
+  }
+  // warp-level combine then one atomic per warp (integer: order-independent)
+  for (int off = 16; off > 0; off >>= 1) {
+    unsigned long long om = __shfl_down_sync(0xffffffffu, my_max, off);
+    unsigned long long os = __shfl_down_sync(0xffffffffu, my_sum, off);
+    my_max = om > my_max ? om : my_max;
+    my_sum += os;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&stats[0], my_max);
+    atomicAdd(&stats[1], my_sum);
+  }
+}
+
+__global__ void row_bin_kernel(int n_rows, const int32_t* __restrict__ rp, int32_t* bin,
+                               int32_t* rows) {
+  for (long long r = gtid(); r < n_rows; r += gstride()) {
+    int len = rp[r + 1] - rp[r];
+    int g = len > 1024 ? 64 : pow2_group(len);  // 64 marks the CTA-per-row bin
+    bin[r] = __ffs(g) - 1;                        // 1..5 for 2..32, 6 for CTA
+    rows[r] = (int32_t)r;
+  }
+}
+
+__global__ void to_fp32_kernel(long long n, const double* __restrict__ a, float* __restrict__ b) {
+  for (long long i = gtid(); i < n; i += gstride()) b[i] = (float)a[i];
+}
+
+template <typename T>
+struct EpiParams {
+  int epi;
+  T alpha, beta;
+  const T* x2;
+  const T* b;
+  double* out;
+  const int* skip;
+  void* partials;
+  int part_off, part_total;
+  bool final_launch;
+  unsigned* counter;
+};
+
+template <typename T>
+__device__ __forceinline__ void row_epilogue(const EpiParams<T>& ep, int row, T s, T* y,
+                                             typename AccOf<T, 1>::type& acc) {
+  if (ep.epi == EPI_AXPBY) {
+    T r = ep.alpha * s;
+    if (ep.beta != T(0)) r = ep.beta * y[row] + r;
+    y[row] = r;
+  } else if (ep.epi == EPI_DOT_X2) {
+    y[row] = s;
+    acc.add_prod(0, ep.x2[row], s);
+  } else {
+    T r = ep.b[row] - s;
+    y[row] = r;
+    acc.add_prod(0, r, r);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void finish_epilogue(const EpiParams<T>& ep,
+                                                typename AccOf<T, 1>::type acc) {
+  typedef typename AccOf<T, 1>::type R;
+  if (ep.epi == EPI_AXPBY) return;
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(ep.partials);
+  if (!ep.final_launch) {
+    if (threadIdx.x == 0) parts[ep.part_off + blockIdx.x] = bs;
+    return;
+  }
+  if (publish_partial(bs, parts, ep.part_off + blockIdx.x, ep.counter, gridDim.x)) {
+    R tot = reduce_partials(parts, ep.part_total);
+    if (threadIdx.x == 0) *ep.out = tot.value(0);
+  }
+}
+
+// G lanes per row; rows either 0..nrows-1 or rows[0..nrows).
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) spmv_group(int nrows, const int32_t* __restrict__ rows,
+                                                     const int32_t* __restrict__ rp,
+                                                     const int32_t* __restrict__ ci,
+                                                     const T* __restrict__ val,
+                                                     const T* __restrict__ x, T* __restrict__ y,
+                                                     EpiParams<T> ep) {
+  if (ep.skip && *ep.skip) return;
+  typedef typename AccOf<T, 1>::type R;
+  R acc = R::zero();
+  constexpr int GPB = kBlock / G;
+  const int gl = threadIdx.x % G;
+  for (long long base = (long long)blockIdx.x * GPB; base < nrows; base += (long long)gridDim.x * GPB) {
+    const long long gid = base + threadIdx.x / G;
+    T s = T(0);
+    int row = -1;
+    if (gid < nrows) {
+      row = rows ? rows[gid] : (int)gid;
+      const int b = rp[row], e = rp[row + 1];
+      for (int j = b + gl; j < e; j += G) s += val[j] * __ldg(x + ci[j]);
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (gl == 0 && row >= 0) row_epilogue(ep, row, s, y, acc);
+  }
+  finish_epilogue(ep, acc);
+}
+
+// One CTA per row (rows longer than 1024 entries).
+template <typename T>
+__global__ void __launch_bounds__(kBlock) spmv_cta(int nrows, const int32_t* __restrict__ rows,
+                                                   const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ ci,
+                                                   const T* __restrict__ val,
+                                                   const T* __restrict__ x, T* __restrict__ y,
+                                                   EpiParams<T> ep) {
+  if (ep.skip && *ep.skip) return;
+  typedef typename AccOf<T, 1>::type R;
+  typedef typename AccOf<T, 1>::type RS;
+  R acc = R::zero();
+  for (long long g = blockIdx.x; g < nrows; g += gridDim.x) {
+    const int row = rows ? rows[g] : (int)g;
+    const int b = rp[row], e = rp[row + 1];
+    Sum<1> part = Sum<1>::zero();
+    T s = T(0);
+    for (int j = b + threadIdx.x; j < e; j += kBlock) s += val[j] * __ldg(x + ci[j]);
+    part.v[0] = (double)s;
+    Sum<1> tot = block_reduce(part);
+    __shared__ T row_sum;
+    if (threadIdx.x == 0) row_sum = (T)tot.v[0];
+    __syncthreads();
+    if (threadIdx.x == 0) row_epilogue(ep, row, row_sum, y, acc);
+    __syncthreads();
+  }
+  (void)sizeof(RS);
+  finish_epilogue(ep, acc);
+}
+
+template <typename T>
+void launch_group(int G, int grid, cudaStream_t st, int nrows, const int32_t* rows,
+                  const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y,
+                  const EpiParams<T>& ep) {
+  switch (G) {
+    case 2: spmv_group<T, 2><<<grid, kBlock, 0, st>>>(nrows, rows, rp, ci, v, x, y, ep); break;
+    case 4: spmv_group<T, 4><<<grid, kBlock, 0, st>>>(nrows, rows, rp, ci, v, x, y, ep); break;
+    case 8: spmv_group<T, 8><<<grid, kBlock, 0, st>>>(nrows, rows, rp, ci, v, x, y, ep); break;
+    case 16: spmv_group<T, 16><<<grid, kBlock, 0, st>>>(nrows, rows, rp, ci, v, x, y, ep); break;
+    case 32: spmv_group<T, 32><<<grid, kBlock, 0, st>>>(nrows, rows, rp, ci, v, x, y, ep); break;
+    default: spmv_cta<T><<<grid, kBlock, 0, st>>>(nrows, rows, rp, ci, v, x, y, ep); break;
+  }
+}
+
+int grid_for(Ctx* ctx, long long items_per_block_unit, long long count) {
+  long long need = (count + items_per_block_unit - 1) / items_per_block_unit;
+  long long cap = (long long)ctx->num_sms * 8;  // 8 resident 256-thread CTAs per SM
+  if (need > cap) need = cap;
+  if (need < 1) need = 1;
+  return (int)need;
+}
+
+}  // namespace
+
+int sm_count(Ctx* ctx) { return ctx->num_sms; }
+unsigned* counter_slot(Ctx* ctx, int i) { return ctx->d_counters + i; }
+
+mtlgpu_status csr_analyse(Csr* A) {
+  Ctx* ctx = A->ctx;
+  MTLGPU_TRY(dalloc(ctx, &A->d_diag, A->n_rows));
+  unsigned long long* d_stats = nullptr;
+  MTLGPU_TRY(dalloc(ctx, &d_stats, 2));
+  MTLGPU_TRY_CUDA(ctx, cudaMemsetAsync(d_stats, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  if (A->n_rows > 0) {
+    int grid = grid_for(ctx, kBlock, A->n_rows);
+    csr_analyse_kernel<<<grid, kBlock, 0, ctx->stream>>>(A->n_rows, A->n_cols, A->nnz, A->d_rp,
+                                                        A->d_ci, A->d_diag, d_stats, ctx->d_error);
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  }
+  unsigned long long h_stats[2] = {0, 0};
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h_stats, d_stats, sizeof(h_stats), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+  dfree(ctx, d_stats);
+  MTLGPU_TRY(take_device_error(ctx));
+  A->max_row = (int)h_stats[0];
+  A->mean_row = A->n_rows ? double(h_stats[1]) / A->n_rows : 0.0;
+
+  int g = 2;
+  while (g < A->mean_row && g < 32) g <<= 1;
+  A->uniform_group = g;
+  A->uniform = A->max_row <= 2 * g || A->max_row <= 32;
+  if (A->uniform) {
+    if (A->max_row <= 32 && A->max_row > 2 * g) {
+      while (g < A->max_row) g <<= 1;
+      A->uniform_group = g;
+    }
+    A->bins.clear();
+    return MTLGPU_OK;
+  }
+  // Binned: stable sort of rows by bin id (cub radix sort keeps equal keys in
+  // input order, so rows inside a bin stay ascending).
+  int n = A->n_rows;
+  int32_t *d_bin = nullptr, *d_rows = nullptr, *d_bin_sorted = nullptr;
+  MTLGPU_TRY(dalloc(ctx, &d_bin, n));
+  MTLGPU_TRY(dalloc(ctx, &d_rows, n));
+  MTLGPU_TRY(dalloc(ctx, &d_bin_sorted, n));
+  MTLGPU_TRY(dalloc(ctx, &A->d_bin_rows, n));
+  row_bin_kernel<<<grid_for(ctx, kBlock, n), kBlock, 0, ctx->stream>>>(n, A->d_rp, d_bin, d_rows);
+  size_t tmp_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_bin, d_bin_sorted, d_rows, A->d_bin_rows, n,
+                                  0, 3, ctx->stream);
+  void* d_tmp = nullptr;
+  MTLGPU_TRY(dalloc(ctx, reinterpret_cast<char**>(&d_tmp), tmp_bytes));
+  cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_bin, d_bin_sorted, d_rows, A->d_bin_rows, n,
+                                  0, 3, ctx->stream);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  std::vector<int32_t> h_bins(n);
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h_bins.data(), d_bin_sorted, sizeof(int32_t) * n,
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+  MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_tmp);
+  dfree(ctx, d_bin);
+  dfree(ctx, d_rows);
+  dfree(ctx, d_bin_sorted);
+  A->bins.clear();
+  int i = 0;
+  while (i < n) {
+    int b = h_bins[i], j = i;
+    while (j < n && h_bins[j] == b) j++;
+    SpmvBin bin;
+    bin.group = b >= 6 ? 0 : (1 << b);
+    bin.begin = i;
+    bin.count = j - i;
+    A->bins.push_back(bin);
+    i = j;
+  }
+  return MTLGPU_OK;
+}
+
+mtlgpu_status csr_ensure_fp32(Csr* A) {
+  if (A->d_v32 || A->nnz == 0) return MTLGPU_OK;
+  Ctx* ctx = A->ctx;
+  MTLGPU_TRY(dalloc(ctx, &A->d_v32, A->nnz));
+  to_fp32_kernel<<<grid_for(ctx, kBlock, A->nnz), kBlock, 0, ctx->stream>>>(A->nnz, A->d_v,
+                                                                            A->d_v32);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+template <typename T>
+const T* csr_values(Csr* A);
+template <>
+const double* csr_values<double>(Csr* A) { return A->d_v; }
+template <>
+const float* csr_values<float>(Csr* A) { return A->d_v32; }
+
+template <typename T>
+mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args) {
+  Ctx* ctx = A->ctx;
+  if (A->n_rows == 0) return MTLGPU_OK;
+  const T* v = csr_values<T>(A);
+  if (!v && A->nnz > 0) return MTLGPU_INVALID_ARG;
+  EpiParams<T> ep;
+  ep.epi = args.epi;
+  ep.alpha = (T)args.alpha;
+  ep.beta = (T)args.beta;
+  ep.x2 = static_cast<const T*>(args.x2);
+  ep.b = static_cast<const T*>(args.b);
+  ep.out = args.out;
+  ep.skip = args.skip;
+  ep.partials = ctx->d_partials;
+  ep.counter = counter_slot(ctx, 0);
+  const int rpg = std::max(1, A->tuned_rows_per_group);
+  (void)rpg;
+  if (A->uniform) {
+    const int G = A->uniform_group;
+    int grid = grid_for(ctx, kBlock / G, A->n_rows);
+    ep.part_off = 0;
+    ep.part_total = grid;
+    ep.final_launch = true;
+    launch_group<T>(G, grid, ctx->stream, A->n_rows, nullptr, A->d_rp, A->d_ci, v, x, y, ep);
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    return MTLGPU_OK;
+  }
+  // binned: partial slots are laid out bin after bin; the last launch reduces all
+  std::vector<int> grids(A->bins.size());
+  int total = 0;
+  for (size_t k = 0; k < A->bins.size(); k++) {
+    const SpmvBin& bn = A->bins[k];
+    int per = bn.group ? kBlock / bn.group : 1;
+    grids[k] = grid_for(ctx, per, bn.count);
+    total += grids[k];
+  }
+  if (total > kMaxPartials) return MTLGPU_NOT_SUPPORTED;
+  int off = 0;
+  for (size_t k = 0; k < A->bins.size(); k++) {
+    const SpmvBin& bn = A->bins[k];
+    ep.part_off = off;
+    ep.part_total = total;
+    ep.final_launch = (k + 1 == A->bins.size());
+    launch_group<T>(bn.group, grids[k], ctx->stream, bn.count, A->d_bin_rows + bn.begin, A->d_rp,
+                    A->d_ci, v, x, y, ep);
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    off += grids[k];
+  }
+  return MTLGPU_OK;
+}
+
+template mtlgpu_status spmv_launch<double>(Csr*, const double*, double*, const SpmvArgs&);
+template mtlgpu_status spmv_launch<float>(Csr*, const float*, float*, const SpmvArgs&);
+
+mtlgpu_status spmv_transposed_launch(Csr* A, const double* x, double* y) {
+  MTLGPU_TRY(csr_ensure_transpose(A));
+  Ctx* ctx = A->ctx;
+  if (A->n_cols == 0) return MTLGPU_OK;
+  EpiParams<double> ep{};
+  ep.epi = EPI_AXPBY;
+  ep.alpha = 1.0;
+  ep.beta = 0.0;
+  ep.partials = ctx->d_partials;
+  ep.counter = counter_slot(ctx, 0);
+  ep.final_launch = true;
+  int G = A->uniform_group;
+  int grid = grid_for(ctx, kBlock / G, A->n_cols);
+  launch_group<double>(G, grid, ctx->stream, A->n_cols, nullptr, A->d_trp, A->d_tci, A->d_tv, x, y,
+                       ep);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+}  // namespace mtlgpu

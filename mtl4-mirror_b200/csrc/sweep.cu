@@ -1,0 +1,139 @@
+// Sync-free triangular sweeps for sm_100a.
+//
+// Replaces the sequential row loops lower_trisolve_t::apply(int_<5>) (unit
+// diagonal, mtl/operation/lower_trisolve.hpp:173-189), apply(int_<6>)
+// (inverted diagonal stored last, 192-209) and upper_trisolve_t::apply(
+// int_<3>) (inverted diagonal stored first, mtl/operation/upper_trisolve.hpp:
+// 160-176, row_update 101-103):
+//     w[r] = (v[r] - sum_j F[r][j] * w[j]) * dia[r]      (dia = 1 for v5)
+//
+// One launch per sweep.  The factor is stored in level order (SweepPlan);
+// warps claim tasks (<= 32/G rows of one level) through an atomic ticket in
+// level order, G lanes per row load the row's off-diagonal entries and wait
+// for each dependency w[j] to become final.  w is NaN-boxed (see device.cuh):
+// the output buffer is prefilled with the sentinel and a row's result is
+// published by a single relaxed store, so a dependency costs one L2 round
+// trip and no fence.  Every wait is bounded; on exhaustion the kernel records
+// MTLGPU_TIMEOUT in the context's error word and all waiters drain quickly.
+// Because tasks are claimed in level order, a row only ever waits on rows
+// claimed earlier by running warps, so the sweep needs no co-residency
+// assumption.  The last warp to finish resets the ticket for the next launch.
+#include <algorithm>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace mtlgpu {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kBlock = 256;
+
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock)
+    sweep_kernel(int n_tasks, const int32_t* __restrict__ task_ptr, const int32_t* __restrict__ rp,
+                 const int32_t* __restrict__ ci, const T* __restrict__ val,
+                 const T* __restrict__ dinv, const int32_t* __restrict__ row_of,
+                 const T* __restrict__ in, T* out, unsigned* ticket, int* err, long long limit,
+                 const int* skip, unsigned total_warps) {
+  if (skip && ld_relaxed(skip)) return;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane / G, gl = lane % G;
+  while (true) {
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(ticket, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= (unsigned)n_tasks) break;
+    const int p = task_ptr[t] + sub;
+    const bool valid = p < task_ptr[t + 1];
+    T acc = T(0), rhs = T(0), d = T(1);
+    int row = 0;
+    if (valid) {
+      row = row_of[p];
+      rhs = in[row];
+      if (dinv) d = dinv[p];
+      const int b = rp[p], e = rp[p + 1];
+      for (int j = b + gl; j < e; j += G) {
+        const int c = ci[j];
+        const T a = val[j];
+        acc += a * wait_value(out + c, limit, err);
+      }
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (valid && gl == 0) {
+      T res = rhs - acc;
+      if (dinv) res = res * d;
+      st_relaxed(out + row, canonical(res));
+    }
+  }
+  if (lane == 0) {
+    __threadfence();
+    unsigned prev = atomicAdd(ticket + 1, 1u);
+    if (prev == total_warps - 1) {
+      ticket[0] = 0;
+      ticket[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
+template <typename T>
+struct PlanVals;
+template <>
+struct PlanVals<double> {
+  static const double* val(const SweepPlan& P) { return P.d_val; }
+  static const double* dinv(const SweepPlan& P) { return P.d_dinv; }
+};
+template <>
+struct PlanVals<float> {
+  static const float* val(const SweepPlan& P) { return P.d_val32; }
+  static const float* dinv(const SweepPlan& P) { return P.d_dinv32; }
+};
+
+}  // namespace
+
+template <typename T>
+mtlgpu_status sweep_launch(Ctx* ctx, const SweepPlan& P, const T* in, T* out, bool prefilled,
+                           const int* skip) {
+  if (P.n == 0) return MTLGPU_OK;
+  const T* val = PlanVals<T>::val(P);
+  const T* dinv = PlanVals<T>::dinv(P);
+  if ((P.nnz_off > 0 && !val) || (!P.unit_diag && !dinv)) return MTLGPU_INVALID_ARG;
+  if (!prefilled) MTLGPU_TRY(fill_sentinel<T>(ctx, out, P.n));
+  const int R = 32 / P.group;
+  long long warps_needed = (P.n_tasks + 0ll);
+  long long max_warps = (long long)ctx->num_sms * (2048 / 32);
+  long long warps = std::max(1ll, std::min(warps_needed, max_warps));
+  int grid = (int)((warps * 32 + kBlock - 1) / kBlock);
+  unsigned total_warps = (unsigned)(grid * (kBlock / 32));
+  (void)R;
+#define MTLGPU_SWEEP_CASE(GG)                                                                   \
+  case GG:                                                                                      \
+    sweep_kernel<T, GG><<<grid, kBlock, 0, ctx->stream>>>(                                      \
+        P.n_tasks, P.d_task_ptr, P.d_rp, P.d_ci, val, dinv, P.d_row_of, in, out, P.d_ticket,    \
+        ctx->d_error, ctx->spin_limit, skip, total_warps);                                      \
+    break;
+  switch (P.group) {
+    MTLGPU_SWEEP_CASE(1)
+    MTLGPU_SWEEP_CASE(2)
+    MTLGPU_SWEEP_CASE(4)
+    MTLGPU_SWEEP_CASE(8)
+    MTLGPU_SWEEP_CASE(16)
+    MTLGPU_SWEEP_CASE(32)
+    default:
+      return MTLGPU_INVALID_ARG;
+  }
+#undef MTLGPU_SWEEP_CASE
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+template mtlgpu_status sweep_launch<double>(Ctx*, const SweepPlan&, const double*, double*, bool,
+                                            const int*);
+template mtlgpu_status sweep_launch<float>(Ctx*, const SweepPlan&, const float*, float*, bool,
+                                           const int*);
+
+}  // namespace mtlgpu

@@ -1,0 +1,408 @@
+"""ctypes binding of libmtlgpu's C ABI (include/mtlgpu.h, include/mtlgpu_fixtures.h).
+
+This is the binding a Python caller of the library uses; the tests and the
+benchmark drive the library through it, so every call crosses the same C
+boundary a C, C++ or FFI user crosses.  Device buffers are ``DeviceArray``
+objects (memory from ``mtlgpu_malloc``); numpy arrays are host buffers.
+
+The library must be built (``make -C mtl4-mirror_b200``); loading fails
+loudly otherwise -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libmtlgpu.so")
+
+OK, MAX_ITER, INVALID_ARG, NOT_SQUARE, MISSING_DIAGONAL, ZERO_PIVOT, BREAKDOWN, TIMEOUT, \
+    INTERRUPTED, CUDA_ERROR, NOT_SORTED, INDEX_RANGE, OUT_OF_MEMORY, INCOMPATIBLE_SIZE, \
+    NOT_SUPPORTED = range(15)
+FP64, FP32 = 0, 1
+PC_IDENTITY, PC_DIAGONAL, PC_ILU0, PC_IC0 = range(4)
+PC_KINDS = {"identity": PC_IDENTITY, "diagonal": PC_DIAGONAL, "ilu0": PC_ILU0, "ic0": PC_IC0}
+CG, BICGSTAB = 0, 1
+METHODS = {"cg": CG, "bicgstab": BICGSTAB}
+SOLVE_FP64, SOLVE_MIXED = 0, 1
+LOWER, UPPER = 0, 1
+
+_vp = C.c_void_p
+
+
+class MtlgpuError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = _lib().mtlgpu_status_string(status).decode() if _LIB else str(status)
+        super().__init__(f"{what}: {msg} ({status})" if what else f"{msg} ({status})")
+
+
+class IterParams(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("rtol", C.c_double), ("atol", C.c_double),
+                ("norm_r0", C.c_double), ("mode", C.c_int), ("inner_rtol", C.c_double),
+                ("inner_max_iter", C.c_int), ("max_outer", C.c_int),
+                ("h_resid_history", C.POINTER(C.c_double)), ("history_cap", C.c_int),
+                ("h_interrupt", C.POINTER(C.c_int))]
+
+
+class IterResult(C.Structure):
+    _fields_ = [("error", C.c_int), ("status", C.c_int), ("iterations", C.c_int),
+                ("outer_iterations", C.c_int), ("resid", C.c_double), ("norm_r0", C.c_double),
+                ("true_resid", C.c_double), ("history_len", C.c_int)]
+
+
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"libmtlgpu not built: {LIB_PATH} missing (make -C mtl4-mirror_b200)")
+        L = C.CDLL(LIB_PATH)
+        L.mtlgpu_status_string.restype = C.c_char_p
+        L.mtlgpu_last_error.restype = C.c_char_p
+        L.mtlgpu_ctx_stream.restype = _vp
+        for name in ("mtlgpu_gen_laplacian2d", "mtlgpu_gen_laplacian3d", "mtlgpu_gen_convdiff27",
+                     "mtlgpu_gen_random_graph", "mtlgpu_gen_fv2d", "mtlgpu_gen_graph_batch"):
+            getattr(L, name).restype = C.c_longlong
+        L.mtlgpu_gen_convdiff27.argtypes = [C.c_int, C.c_uint64, _vp, _vp, _vp]
+        L.mtlgpu_gen_random_graph.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, _vp,
+                                              _vp, _vp]
+        L.mtlgpu_gen_fv2d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, _vp, _vp, _vp]
+        L.mtlgpu_gen_graph_batch.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                             C.c_double, C.c_uint64, _vp, _vp, _vp, _vp]
+        L.mtlgpu_gen_uniform.argtypes = [C.c_longlong, C.c_uint64, C.c_double, C.c_double, _vp]
+        L.mtlgpu_gen_normal.argtypes = [C.c_longlong, C.c_uint64, _vp]
+        L.mtlgpu_ctx_set_spin_limit.argtypes = [_vp, C.c_longlong]
+        L.mtlgpu_malloc.argtypes = [_vp, C.c_size_t, C.POINTER(_vp)]
+        L.mtlgpu_free.argtypes = [_vp, _vp]
+        L.mtlgpu_memcpy_h2d.argtypes = [_vp, _vp, _vp, C.c_size_t]
+        L.mtlgpu_memcpy_d2h.argtypes = [_vp, _vp, _vp, C.c_size_t]
+        L.mtlgpu_spmv.argtypes = [_vp, _vp, _vp, C.c_double, C.c_double]
+        L.mtlgpu_axpy.argtypes = [_vp, C.c_int, C.c_double, _vp, _vp]
+        L.mtlgpu_xpay.argtypes = [_vp, C.c_int, _vp, C.c_double, _vp]
+        L.mtlgpu_dot.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(C.c_double)]
+        L.mtlgpu_two_norm.argtypes = [_vp, C.c_int, _vp, C.POINTER(C.c_double)]
+        L.mtlgpu_unary_dot.argtypes = [_vp, C.c_int, _vp, C.POINTER(C.c_double)]
+        _LIB = L
+    return _LIB
+
+
+def lib():
+    return _lib()
+
+
+def check(status, what=""):
+    if status != OK:
+        raise MtlgpuError(status, what)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+# ---------------------------------------------------------------------------
+class Context:
+    def __init__(self, device=0, stream=None):
+        self.h = _vp()
+        if stream is None:
+            check(_lib().mtlgpu_ctx_create(device, C.byref(self.h)), "ctx_create")
+        else:
+            check(_lib().mtlgpu_ctx_create_on_stream(device, _vp(stream), C.byref(self.h)),
+                  "ctx_create_on_stream")
+
+    @property
+    def stream(self):
+        return _lib().mtlgpu_ctx_stream(self.h)
+
+    def synchronize(self):
+        check(_lib().mtlgpu_ctx_synchronize(self.h))
+
+    def set_spin_limit(self, polls):
+        check(_lib().mtlgpu_ctx_set_spin_limit(self.h, int(polls)))
+
+    def last_error(self):
+        return _lib().mtlgpu_last_error(self.h).decode()
+
+    def close(self):
+        if self.h:
+            _lib().mtlgpu_ctx_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # device memory -------------------------------------------------------
+    def array(self, n, dtype=np.float64):
+        return DeviceArray(self, n, dtype)
+
+    def to_device(self, a):
+        a = np.ascontiguousarray(a)
+        d = DeviceArray(self, a.size, a.dtype)
+        d.upload(a)
+        return d
+
+    def dot(self, x, y):
+        r = C.c_double()
+        check(_lib().mtlgpu_dot(self.h, x.n, x.ptr, y.ptr, C.byref(r)), "dot")
+        return r.value
+
+    def two_norm(self, x):
+        r = C.c_double()
+        check(_lib().mtlgpu_two_norm(self.h, x.n, x.ptr, C.byref(r)), "two_norm")
+        return r.value
+
+    def unary_dot(self, x):
+        r = C.c_double()
+        check(_lib().mtlgpu_unary_dot(self.h, x.n, x.ptr, C.byref(r)), "unary_dot")
+        return r.value
+
+    def axpy(self, alpha, x, y):
+        check(_lib().mtlgpu_axpy(self.h, x.n, float(alpha), x.ptr, y.ptr), "axpy")
+
+    def xpay(self, x, beta, y):
+        check(_lib().mtlgpu_xpay(self.h, x.n, x.ptr, float(beta), y.ptr), "xpay")
+
+
+class DeviceArray:
+    def __init__(self, ctx, n, dtype=np.float64):
+        self.ctx = ctx
+        self.n = int(n)
+        self.dtype = np.dtype(dtype)
+        self.ptr = _vp()
+        check(_lib().mtlgpu_malloc(ctx.h, max(1, self.n) * self.dtype.itemsize,
+                                   C.byref(self.ptr)), "malloc")
+
+    @property
+    def nbytes(self):
+        return self.n * self.dtype.itemsize
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, self.dtype)
+        assert a.size == self.n
+        check(_lib().mtlgpu_memcpy_h2d(self.ctx.h, self.ptr, _p(a), self.nbytes), "h2d")
+
+    def download(self, out=None):
+        out = np.empty(self.n, self.dtype) if out is None else out
+        check(_lib().mtlgpu_memcpy_d2h(self.ctx.h, _p(out), self.ptr, self.nbytes), "d2h")
+        return out
+
+    def free(self):
+        if self.ptr:
+            _lib().mtlgpu_free(self.ctx.h, self.ptr)
+            self.ptr = _vp()
+
+    def __del__(self):
+        try:
+            if self.ctx.h:
+                self.free()
+        except Exception:
+            pass
+
+
+class Csr:
+    """Device CSR handle (replaces compressed2D on the solve path)."""
+
+    def __init__(self, ctx, rp, ci, v, n_cols=None):
+        self.ctx = ctx
+        rp = np.ascontiguousarray(rp, np.int32)
+        ci = np.ascontiguousarray(ci, np.int32)
+        v = np.ascontiguousarray(v, np.float64)
+        self.n = len(rp) - 1
+        self.n_cols = self.n if n_cols is None else n_cols
+        self.nnz = len(ci)
+        self.h = _vp()
+        st = _lib().mtlgpu_csr_create(ctx.h, self.n, self.n_cols, self.nnz, _p(rp), _p(ci), _p(v),
+                                      C.byref(self.h))
+        check(st, "csr_create")
+
+    def set_values(self, v):
+        v = np.ascontiguousarray(v, np.float64)
+        check(_lib().mtlgpu_csr_set_values(self.h, _p(v), None), "csr_set_values")
+
+    def spmv(self, x, y, alpha=1.0, beta=0.0):
+        check(_lib().mtlgpu_spmv(self.h, x.ptr, y.ptr, float(alpha), float(beta)), "spmv")
+
+    def spmv_transposed(self, x, y):
+        check(_lib().mtlgpu_spmv_transposed(self.h, x.ptr, y.ptr), "spmv_transposed")
+
+    def autotune(self):
+        c = C.c_int()
+        check(_lib().mtlgpu_csr_autotune(self.h, C.byref(c)), "autotune")
+        return c.value
+
+    def close(self):
+        if self.h:
+            _lib().mtlgpu_csr_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            if self.ctx.h:
+                self.close()
+        except Exception:
+            pass
+
+
+class Pc:
+    """Preconditioner handle (itl::pc::identity / diagonal / ilu_0 / ic_0)."""
+
+    def __init__(self, A, kind, prec=FP64, allow_pivot=True):
+        self.A = A
+        self.kind = PC_KINDS.get(kind, kind)
+        self.prec = prec
+        self.h = _vp()
+        st = _lib().mtlgpu_pc_create(A.h, self.kind, prec, C.byref(self.h))
+        self.status = st
+        if st != OK and not (allow_pivot and st == ZERO_PIVOT and self.h):
+            raise MtlgpuError(st, "pc_create")
+
+    def apply(self, r, z):
+        check(_lib().mtlgpu_pc_apply(self.h, r.ptr, z.ptr), "pc_apply")
+
+    def adjoint_apply(self, r, z):
+        check(_lib().mtlgpu_pc_adjoint_apply(self.h, r.ptr, z.ptr), "pc_adjoint_apply")
+
+    def sweep(self, which, x, y):
+        check(_lib().mtlgpu_pc_sweep(self.h, which, x.ptr, y.ptr), "pc_sweep")
+
+    def factor_info(self, which):
+        nnz, lev = C.c_int(), C.c_int()
+        check(_lib().mtlgpu_pc_factor_info(self.h, which, C.byref(nnz), C.byref(lev)))
+        return nnz.value, lev.value
+
+    def factor(self, which):
+        nnz, _ = self.factor_info(which)
+        n = self.A.n
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(max(nnz, 1), np.int32)
+        v = np.zeros(max(nnz, 1))
+        check(_lib().mtlgpu_pc_get_factor(self.h, which, _p(rp), _p(ci), _p(v)), "get_factor")
+        return (n, rp, ci[:nnz], v[:nnz])
+
+    def levels(self, which):
+        lev = np.zeros(self.A.n, np.int32)
+        check(_lib().mtlgpu_pc_get_levels(self.h, which, _p(lev)), "get_levels")
+        return lev
+
+    def close(self):
+        if self.h:
+            _lib().mtlgpu_pc_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            if self.A.ctx.h and self.A.h:
+                self.close()
+        except Exception:
+            pass
+
+
+def make_params(max_iter=1000, rtol=1e-10, atol=0.0, norm_r0=-1.0, mode=SOLVE_FP64,
+                inner_rtol=1e-4, inner_max_iter=0, max_outer=0, history=None, interrupt=None):
+    p = IterParams()
+    _lib().mtlgpu_iter_params_default(C.byref(p))
+    p.max_iter, p.rtol, p.atol, p.norm_r0, p.mode = max_iter, rtol, atol, norm_r0, mode
+    p.inner_rtol, p.inner_max_iter, p.max_outer = inner_rtol, inner_max_iter, max_outer
+    if history is not None:
+        p.h_resid_history = history.ctypes.data_as(C.POINTER(C.c_double))
+        p.history_cap = len(history)
+    if interrupt is not None:
+        p.h_interrupt = interrupt.ctypes.data_as(C.POINTER(C.c_int))
+    return p
+
+
+def solve(method, A, P, x, b, **kw):
+    """itl::cg / itl::bicgstab on device arrays; returns (status, IterResult, history)."""
+    hist = np.zeros(2 * kw.get("max_iter", 1000) + 8)
+    prm = make_params(history=hist, **kw)
+    res = IterResult()
+    st = _lib().mtlgpu_solve(METHODS.get(method, method), A.h, P.h if P else None, x.ptr, b.ptr,
+                             C.byref(prm), C.byref(res))
+    return st, res, hist[:min(res.history_len, len(hist))].copy()
+
+
+def solve_host(method, A, P, x, b, **kw):
+    """Same with host numpy x (updated in place) and b."""
+    hist = np.zeros(2 * kw.get("max_iter", 1000) + 8)
+    prm = make_params(history=hist, **kw)
+    res = IterResult()
+    x = np.ascontiguousarray(x, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    st = _lib().mtlgpu_solve_host(METHODS.get(method, method), A.h, P.h if P else None, _p(x),
+                                  _p(b), C.byref(prm), C.byref(res))
+    return st, res, x
+
+
+# ---------------------------------------------------------------------------
+# fixtures (host generators)
+def _two_phase(fn, *args):
+    nnz = fn(*args, None, None, None)
+    return nnz
+
+
+def laplacian2d(m, n):
+    L = _lib()
+    nnz = L.mtlgpu_gen_laplacian2d(m, n, None, None, None)
+    rp, ci, v = np.zeros(m * n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.mtlgpu_gen_laplacian2d(m, n, _p(rp), _p(ci), _p(v))
+    return (m * n, rp, ci, v)
+
+
+def laplacian3d(N):
+    L = _lib()
+    nnz = L.mtlgpu_gen_laplacian3d(N, None, None, None)
+    rp, ci, v = np.zeros(N ** 3 + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.mtlgpu_gen_laplacian3d(N, _p(rp), _p(ci), _p(v))
+    return (N ** 3, rp, ci, v)
+
+
+def convdiff27(N, seed=2):
+    L = _lib()
+    nnz = L.mtlgpu_gen_convdiff27(N, seed, None, None, None)
+    rp, ci, v = np.zeros(N ** 3 + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.mtlgpu_gen_convdiff27(N, seed, _p(rp), _p(ci), _p(v))
+    return (N ** 3, rp, ci, v)
+
+
+def random_graph(n, avg_deg, shift_frac=1e-2, seed=3):
+    L = _lib()
+    nnz = L.mtlgpu_gen_random_graph(n, avg_deg, shift_frac, seed, None, None, None)
+    rp, ci, v = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.mtlgpu_gen_random_graph(n, avg_deg, shift_frac, seed, _p(rp), _p(ci), _p(v))
+    return (n, rp, ci, v)
+
+
+def fv2d(N, sigma=1.0, corr=8.0, seed=4):
+    L = _lib()
+    nnz = L.mtlgpu_gen_fv2d(N, sigma, corr, seed, None, None, None)
+    rp, ci, v = np.zeros(N * N + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.mtlgpu_gen_fv2d(N, sigma, corr, seed, _p(rp), _p(ci), _p(v))
+    return (N * N, rp, ci, v)
+
+
+def uniform(n, seed, a=-1.0, b=1.0):
+    out = np.zeros(n)
+    _lib().mtlgpu_gen_uniform(n, seed, a, b, _p(out))
+    return out
+
+
+def normal(n, seed):
+    out = np.zeros(n)
+    _lib().mtlgpu_gen_normal(n, seed, _p(out))
+    return out
+
+
+def csr_mult(A, x):
+    n, rp, ci, v = A
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.zeros(n)
+    _lib().mtlgpu_gen_csr_mult(n, _p(rp), _p(ci), _p(v), _p(x), _p(y))
+    return y

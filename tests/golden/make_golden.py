@@ -1,0 +1,139 @@
+"""Generates tests/golden/golden.npz from the MTL4 reference itself.
+
+Run in a checkout where the reference tree is present (it is compiled by
+``make -C oracle``; the library it produces is ``oracle/_ref/libmtlref.so``):
+
+    python tests/golden/make_golden.py            # small cases (seconds)
+    python tests/golden/make_golden.py --cfg2     # + the 128^3 solve (about a minute)
+
+Every array stored here is an output of the reference's own code path
+(laplacian_setup, compressed2D SpMV, ic_0 / ilu_0 factors, solve(P, x),
+itl::cg / itl::bicgstab with basic_iteration), except the level arrays,
+which the reference does not compute: those come from the restatement
+(oracle/restate.c, or_levels_lower/upper) applied to the reference's own
+factor patterns.  Inputs come from the library's seeded generators
+(include/mtlgpu_fixtures.h).
+"""
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "mtl4-mirror_b200", "python"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import mtlgpu as M  # noqa: E402
+import oracle as O  # noqa: E402
+
+
+def put_csr(out, key, A):
+    out[key + "_rp"], out[key + "_ci"], out[key + "_v"] = A[1], A[2], A[3]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cfg2", action="store_true")
+    args = ap.parse_args()
+    R = O.Reference()
+    S = O.Restatement()
+    out = {}
+
+    # ic_0_test.cpp: 3x3 grid, ic_0<M, float>, y = solve(P, iota)
+    A3 = R.laplacian_setup(3, 3)
+    out["kat_ic0_float_iota"] = R.pc_apply("ic0_float", A3, np.arange(9.0))
+
+    # config 1: 100x100 Laplacian, x_true ~ U[-1,1] seed 0, cg + ic_0 to 1e-10
+    A1 = R.laplacian_setup(100, 100)
+    xt = M.uniform(A1[0], 0)
+    b1 = R.spmv(A1, xt)
+    r = R.solve("cg", "ic0", A1, b1, rtol=1e-10, max_iter=1000)
+    out["cfg1_b"], out["cfg1_x"], out["cfg1_hist"] = b1, r["x"], r["history"]
+    out["cfg1_iters"] = np.array([r["iterations"], r["err"]])
+    for pc in ("identity", "diagonal", "ilu0"):
+        rr = R.solve("cg", pc, A1, b1, rtol=1e-10, max_iter=1000)
+        out[f"cfg1_{pc}_iters"] = np.array([rr["iterations"], rr["err"]])
+        out[f"cfg1_{pc}_hist"] = rr["history"]
+    L, U = R.ic0(A1)
+    out["cfg1_ic0_L_v"], out["cfg1_ic0_U_v"] = L[3], U[3]
+    out["cfg1_ic0_L_lev"] = S.levels(L, True)[0]
+    out["cfg1_ic0_U_lev"] = S.levels(U, False)[0]
+
+    # 3-D 7-point, 16^3 (x_true seed 1)
+    A = M.laplacian3d(16)
+    xt = M.uniform(A[0], 1)
+    b = R.spmv(A, xt)
+    r = R.solve("cg", "ic0", A, b, rtol=1e-10, max_iter=2000)
+    out["lap16_b"], out["lap16_hist"] = b, r["history"]
+    out["lap16_iters"] = np.array([r["iterations"], r["err"]])
+    L, U = R.ic0(A)
+    put_csr(out, "lap16_ic0_L", L)
+    put_csr(out, "lap16_ic0_U", U)
+    out["lap16_ic0_L_lev"] = S.levels(L, True)[0]
+    out["lap16_ic0_U_lev"] = S.levels(U, False)[0]
+    Lf, Uf = R.ic0(A, as_float=True)
+    out["lap16_ic0f_U_v"] = Uf[3]
+    out["lap16_pc_ic0_apply"] = R.pc_apply("ic0", A, b)
+
+    # 27-point convection-diffusion, 8^3 (seed 2): bicgstab + ilu_0
+    A = M.convdiff27(8, 2)
+    xt = M.uniform(A[0], 1)
+    b = R.spmv(A, xt)
+    r = R.solve("bicgstab", "ilu0", A, b, rtol=1e-10, max_iter=1000)
+    out["cd8_b"], out["cd8_hist"], out["cd8_x"] = b, r["history"], r["x"]
+    out["cd8_iters"] = np.array([r["iterations"], r["err"]])
+    L, U = R.ilu0(A)
+    put_csr(out, "cd8_ilu0_L", L)
+    put_csr(out, "cd8_ilu0_U", U)
+    out["cd8_ilu0_L_lev"] = S.levels(L, True)[0]
+    out["cd8_ilu0_U_lev"] = S.levels(U, False)[0]
+    out["cd8_pc_ilu0_apply"] = R.pc_apply("ilu0", A, b)
+    out["cd8_pc_ilu0_adjoint"] = R.pc_apply("ilu0", A, b, adjoint=True)
+    rr = R.solve("bicgstab", "diagonal", A, b, rtol=1e-10, max_iter=1000)
+    out["cd8_diag_iters"] = np.array([rr["iterations"], rr["err"]])
+
+    # random-graph Laplacian (n = 600, degree 12, seed 3): IC(0) as written
+    A = M.random_graph(600, 12.0, 1e-2, 3)
+    b = M.normal(A[0], 3)
+    L, U = R.ic0(A)
+    put_csr(out, "rg_ic0_L", L)
+    put_csr(out, "rg_ic0_U", U)
+    out["rg_ic0_L_lev"] = S.levels(L, True)[0]
+    out["rg_ic0_U_lev"] = S.levels(U, False)[0]
+    out["rg_b"] = b
+    for pc in ("ic0", "diagonal"):
+        rr = R.solve("cg", pc, A, b, rtol=1e-8, max_iter=1000)
+        out[f"rg_{pc}_iters"] = np.array([rr["iterations"], rr["err"]])
+        out[f"rg_{pc}_hist"] = rr["history"]
+
+    # 2-D finite volume, 32^2 (seed 4)
+    A = M.fv2d(32, 1.0, 8.0, 4)
+    b = M.normal(A[0], 4)
+    rr = R.solve("cg", "ic0", A, b, rtol=1e-10, max_iter=1000)
+    out["fv32_b"] = b
+    out["fv32_iters"] = np.array([rr["iterations"], rr["err"]])
+    out["fv32_hist"] = rr["history"]
+
+    if args.cfg2:
+        A = M.laplacian3d(128)
+        xt = M.uniform(A[0], 1)
+        b = M.csr_mult(A, xt)
+        rr = R.solve("cg", "ic0", A, b, rtol=1e-10, max_iter=2000)
+        out["cfg2_iters"] = np.array([rr["iterations"], rr["err"]])
+        out["cfg2_hist"] = rr["history"]
+    else:
+        old = os.path.join(HERE, "golden.npz")
+        if os.path.exists(old):
+            prev = np.load(old)
+            for k in ("cfg2_iters", "cfg2_hist"):
+                if k in prev:
+                    out[k] = prev[k]
+
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+"""GPU kernels against the oracle, through the C ABI.
+
+Tolerances (stated per test): SpMV normwise relative error <= 1e-14 (FP64);
+factor values bit-identical (the device follows the reference's operation
+order with separate roundings); level arrays bit-exact; one triangular
+sweep / preconditioner apply <= 1e-12 relative (the device sums each row's
+products in a tree, the reference sequentially)."""
+import numpy as np
+import pytest
+
+from helpers import csr_eq, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def matrices(M):
+    return {
+        "lap2d_100": M.laplacian2d(100, 100),
+        "lap3d_20": M.laplacian3d(20),
+        "cd27_10": M.convdiff27(10, 2),
+        "graph_2000": M.random_graph(2000, 20.0, 1e-2, 3),
+        "fv2d_64": M.fv2d(64),
+    }
+
+
+@pytest.mark.parametrize("name", ["lap2d_100", "lap3d_20", "cd27_10", "graph_2000", "fv2d_64"])
+def test_spmv_modes(M, ctx, restate, name):
+    A = matrices(M)[name]
+    n = A[0]
+    dA = M.Csr(ctx, *A[1:])
+    x = M.uniform(n, 5)
+    y0 = M.uniform(n, 6)
+    dx, dy = ctx.to_device(x), ctx.to_device(y0)
+    for mode, (alpha, beta) in enumerate([(1.0, 0.0), (1.0, 1.0), (-1.0, 1.0)]):
+        dy.upload(y0)
+        dA.spmv(dx, dy, alpha, beta)
+        ref = restate.spmv(A, x, y0, mode)
+        assert rel_err(dy.download(), ref) <= 1e-14, (name, mode)
+
+
+def test_spmv_stencil_known_answer(M, ctx):
+    # matrix_vector_product_test.cpp:43-89 on the device
+    A = M.laplacian2d(5, 5)
+    n, rp, ci, v = A
+    row12 = np.zeros(25)
+    row12[ci[rp[12]:rp[13]]] = v[rp[12]:rp[13]]
+    dA = M.Csr(ctx, rp, ci, v)
+    dv, dw = ctx.to_device(row12), ctx.array(25)
+    dA.spmv(dv, dw)
+    w = dw.download()
+    assert (w[12], w[13], w[14], w[15], w[17], w[18], w[22]) == (20, -8, 1, 0, -8, 2, 1)
+    dA.spmv(dv, dw, 1.0, 1.0)
+    w = dw.download()
+    assert w[12] == 40 and w[18] == 4
+    dA.spmv(dv, dw, -1.0, 1.0)
+    w = dw.download()
+    assert w[12] == 20 and w[18] == 2
+
+
+def test_spmv_binned_rows(M, ctx, restate):
+    # rows of very different lengths exercise the row bins, including a
+    # CTA-per-row bin (rows longer than 1024 entries)
+    rng = np.random.default_rng(3)
+    n = 3000
+    lens = rng.integers(0, 12, n)
+    lens[::97] = rng.integers(40, 300, len(lens[::97]))
+    lens[5] = 2500
+    lens[1700] = 1400
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    v = rng.standard_normal(len(ci))
+    A = (n, rp, ci, v)
+    dA = M.Csr(ctx, rp, ci, v)
+    x = rng.standard_normal(n)
+    dx, dy = ctx.to_device(x), ctx.array(n)
+    dA.spmv(dx, dy)
+    assert rel_err(dy.download(), restate.spmv(A, x)) <= 1e-14
+
+
+def test_spmv_transposed(M, ctx):
+    A = M.convdiff27(6, 2)
+    n, rp, ci, v = A
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    D = np.zeros((n, n))
+    D[rows, ci] = v
+    x = M.uniform(n, 9)
+    dA = M.Csr(ctx, rp, ci, v)
+    dx, dy = ctx.to_device(x), ctx.array(n)
+    dA.spmv_transposed(dx, dy)
+    assert rel_err(dy.download(), D.T @ x) <= 1e-14
+
+
+def test_csr_validation(M, ctx):
+    A = M.laplacian2d(4, 4)
+    n, rp, ci, v = A
+    bad = ci.copy()
+    bad[3], bad[4] = bad[4], bad[3]
+    with pytest.raises(M.MtlgpuError) as e:
+        M.Csr(ctx, rp, bad, v)
+    assert e.value.status == M.NOT_SORTED
+    bad = ci.copy()
+    bad[-1] = 99
+    with pytest.raises(M.MtlgpuError) as e:
+        M.Csr(ctx, rp, bad, v)
+    assert e.value.status == M.INDEX_RANGE
+    # empty matrix
+    E = M.Csr(ctx, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    E.close()
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 7, 9, 1000, 100003, 2097152])
+def test_blas1(M, ctx, restate, n):
+    x, y = M.uniform(n, 21), M.uniform(n, 22)
+    dx, dy = ctx.to_device(x), ctx.to_device(y)
+    assert abs(ctx.dot(dx, dy) - restate.dot(x, y)) <= 1e-13 * max(1.0, abs(restate.dot(x, y)))
+    assert abs(ctx.two_norm(dx) - restate.two_norm(x)) <= 1e-14 * restate.two_norm(x)
+    ctx.axpy(0.5, dx, dy)
+    assert np.allclose(dy.download(), y + 0.5 * x, rtol=0, atol=1e-15)
+    dy.upload(y)
+    ctx.xpay(dx, -2.0, dy)
+    assert np.allclose(dy.download(), x - 2.0 * y, rtol=0, atol=1e-15)
+    # determinism: same bits on every call
+    assert ctx.dot(dx, dx) == ctx.dot(dx, dx)
+
+
+def test_dot_known_answer(M, ctx):
+    u = ctx.to_device(np.arange(1.0, 10.0))
+    assert ctx.dot(u, u) == 285.0
+
+
+FACTOR_CASES = ["lap3d_20", "cd27_10", "graph_2000", "fv2d_64", "lap2d_100"]
+
+
+@pytest.mark.parametrize("name", FACTOR_CASES)
+@pytest.mark.parametrize("kind", ["ic0", "ilu0"])
+def test_factors_bit_exact(M, ctx, restate, name, kind):
+    A = matrices(M)[name]
+    if kind == "ic0" and name == "cd27_10":
+        A = M.random_graph(1500, 9.0, 1e-2, 8)   # IC(0) needs a symmetric matrix
+    dA = M.Csr(ctx, *A[1:])
+    P = M.Pc(dA, kind)
+    L, U = getattr(restate, kind)(A)
+    gL, gU = P.factor(M.LOWER), P.factor(M.UPPER)
+    assert csr_eq(gL, L), "L pattern/values differ"
+    assert csr_eq(gU, U), "U pattern/values differ"
+    # level arrays: bit-exact with the levels of the reference's patterns
+    assert np.array_equal(P.levels(M.LOWER), restate.levels(L, True)[0])
+    assert np.array_equal(P.levels(M.UPPER), restate.levels(U, False)[0])
+    nnzL, nlevL = P.factor_info(M.LOWER)
+    assert nnzL == len(L[2]) and nlevL == restate.levels(L, True)[1]
+
+
+def test_factors_against_golden(M, ctx, golden):
+    A = M.laplacian3d(16)
+    P = M.Pc(M.Csr(ctx, *A[1:]), "ic0")
+    for which, key in ((M.LOWER, "lap16_ic0_L"), (M.UPPER, "lap16_ic0_U")):
+        F = P.factor(which)
+        assert csr_eq(F, (F[0], golden[key + "_rp"], golden[key + "_ci"], golden[key + "_v"]))
+    assert np.array_equal(P.levels(M.LOWER), golden["lap16_ic0_L_lev"])
+    assert np.array_equal(P.levels(M.UPPER), golden["lap16_ic0_U_lev"])
+    Pf = M.Pc(M.Csr(ctx, *A[1:]), "ic0", M.FP32)
+    assert np.array_equal(Pf.factor(M.UPPER)[3], golden["lap16_ic0f_U_v"])
+    C = M.convdiff27(8, 2)
+    P = M.Pc(M.Csr(ctx, *C[1:]), "ilu0")
+    for which, key in ((M.LOWER, "cd8_ilu0_L"), (M.UPPER, "cd8_ilu0_U")):
+        F = P.factor(which)
+        assert csr_eq(F, (F[0], golden[key + "_rp"], golden[key + "_ci"], golden[key + "_v"]))
+    assert np.array_equal(P.levels(M.LOWER), golden["cd8_ilu0_L_lev"])
+    G = M.random_graph(600, 12.0, 1e-2, 3)
+    P = M.Pc(M.Csr(ctx, *G[1:]), "ic0")
+    assert np.array_equal(P.factor(M.LOWER)[3], golden["rg_ic0_L_v"])
+    assert np.array_equal(P.factor(M.UPPER)[3], golden["rg_ic0_U_v"])
+
+
+@pytest.mark.parametrize("name", FACTOR_CASES)
+@pytest.mark.parametrize("kind", ["ic0", "ilu0", "diagonal", "identity"])
+def test_pc_apply(M, ctx, restate, name, kind):
+    A = matrices(M)[name]
+    if kind == "ic0" and name == "cd27_10":
+        A = M.random_graph(1500, 9.0, 1e-2, 8)
+    n = A[0]
+    dA = M.Csr(ctx, *A[1:])
+    P = M.Pc(dA, kind)
+    r = M.uniform(n, 31)
+    dr, dz = ctx.to_device(r), ctx.array(n)
+    P.apply(dr, dz)
+    assert rel_err(dz.download(), restate.pc_apply(kind, A, r)) <= 1e-12
+    P.adjoint_apply(dr, dz)
+    assert rel_err(dz.download(), restate.pc_apply(kind, A, r, adjoint=True)) <= 1e-12
+    # a second apply reuses the plans and must give the same bits
+    z1 = dz.download()
+    P.adjoint_apply(dr, dz)
+    assert np.array_equal(z1, dz.download())
+
+
+def test_pc_apply_golden(M, ctx, golden):
+    A = M.laplacian3d(16)
+    P = M.Pc(M.Csr(ctx, *A[1:]), "ic0")
+    db, dz = ctx.to_device(golden["lap16_b"]), ctx.array(A[0])
+    P.apply(db, dz)
+    assert rel_err(dz.download(), golden["lap16_pc_ic0_apply"]) <= 1e-12
+    C = M.convdiff27(8, 2)
+    P = M.Pc(M.Csr(ctx, *C[1:]), "ilu0")
+    db, dz = ctx.to_device(golden["cd8_b"]), ctx.array(C[0])
+    P.apply(db, dz)
+    assert rel_err(dz.download(), golden["cd8_pc_ilu0_apply"]) <= 1e-12
+    P.adjoint_apply(db, dz)
+    assert rel_err(dz.download(), golden["cd8_pc_ilu0_adjoint"]) <= 1e-12
+
+
+def test_single_sweeps(M, ctx, restate):
+    A = M.laplacian3d(12)
+    n = A[0]
+    P = M.Pc(M.Csr(ctx, *A[1:]), "ic0")
+    L, U = restate.ic0(A)
+    r = M.uniform(n, 41)
+    dr, dy = ctx.to_device(r), ctx.array(n)
+    P.sweep(M.LOWER, dr, dy)
+    assert rel_err(dy.download(), restate.sweep("lower_invdiag_last", L, r)) <= 1e-12
+    P.sweep(M.UPPER, dr, dy)
+    assert rel_err(dy.download(), restate.sweep("upper_invdiag_first", U, r)) <= 1e-12
+    C = M.convdiff27(6, 2)
+    Q = M.Pc(M.Csr(ctx, *C[1:]), "ilu0")
+    L, U = restate.ilu0(C)
+    r = M.uniform(C[0], 42)
+    dr, dy = ctx.to_device(r), ctx.array(C[0])
+    Q.sweep(M.LOWER, dr, dy)
+    assert rel_err(dy.download(), restate.sweep("lower_unit", L, r)) <= 1e-12
+
+
+def test_missing_diagonal(M, ctx):
+    A = M.laplacian2d(4, 4)
+    n, rp, ci, v = A
+    keep = np.ones(len(ci), bool)
+    keep[rp[5] + 2] = False  # drop the diagonal of row 5 (5-point order: -n, -1, diag)
+    assert ci[rp[5] + 2] == 5
+    rp2 = np.concatenate([[0], np.cumsum([keep[rp[i]:rp[i + 1]].sum() for i in range(n)])])
+    dA = M.Csr(ctx, rp2.astype(np.int32), ci[keep], v[keep])
+    for kind in ("ic0", "ilu0"):
+        with pytest.raises(M.MtlgpuError) as e:
+            M.Pc(dA, kind)
+        assert e.value.status == M.MISSING_DIAGONAL
+
+
+def test_zero_pivot_reported(M, ctx):
+    # a singular 2x2 block: the factor is still produced (inf), status ZERO_PIVOT
+    rp = np.array([0, 2, 4], np.int32)
+    ci = np.array([0, 1, 0, 1], np.int32)
+    v = np.array([1.0, 1.0, 1.0, 1.0])
+    P = M.Pc(M.Csr(ctx, rp, ci, v), "ilu0")
+    assert P.status == M.ZERO_PIVOT
+    Q = M.Pc(M.Csr(ctx, rp, ci, v), "ic0")
+    assert Q.status == M.ZERO_PIVOT
