@@ -130,6 +130,8 @@ typedef struct {
   double norm_r0;
   double true_resid;     /* ||b - A x||_2 in FP64 at exit */
   int history_len;       /* entries written to h_resid_history */
+  long long kernel_launches; /* device kernels this call launched (graph
+                                nodes counted per graph launch) */
 } mtlgpu_iter_result;
 
 /* ---- context ----------------------------------------------------------- */
@@ -216,6 +218,10 @@ mtlgpu_status mtlgpu_pc_adjoint_apply(mtlgpu_pc* P, const double* d_r, double* d
  * 192-209); MTLGPU_UPPER is upper_trisolve v3 (inverted diagonal first;
  * upper_trisolve.hpp:160-176). */
 mtlgpu_status mtlgpu_pc_sweep(mtlgpu_pc* P, int which, const double* d_in, double* d_out);
+/* The same sweep on float32 vectors with the FP32 factors (preconditioner
+ * created with factor precision MTLGPU_FP32): the sweep the inner solves of
+ * MIXED_REFINED run. */
+mtlgpu_status mtlgpu_pc_sweep_f32(mtlgpu_pc* P, int which, const float* d_in, float* d_out);
 /* Factor sizes and level counts: nnz of the factor as the reference stores it
  * (L of IC(0) includes the diagonal, L of ILU(0) does not). */
 mtlgpu_status mtlgpu_pc_factor_info(const mtlgpu_pc* P, int which, int* nnz, int* n_levels);

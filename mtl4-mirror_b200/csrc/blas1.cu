@@ -76,6 +76,7 @@ mtlgpu_status dot_launch(Ctx* ctx, int n, const double* x, const double* y, doub
     MTLGPU_TRY_CUDA(ctx, cudaMemsetAsync(d_out, 0, sizeof(double), ctx->stream));
     return MTLGPU_OK;
   }
+  ctx->launches++;
   dot_kernel<<<vec_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, x, y, d_out, ctx->d_partials,
                                                            counter_slot(ctx, 8));
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());

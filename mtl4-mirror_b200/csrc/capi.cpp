@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -48,6 +49,7 @@ mtlgpu_status set_device(Ctx* ctx) {
 mtlgpu_status ctx_init(Ctx* ctx) {
   MTLGPU_TRY_CUDA(ctx, cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount,
                                               ctx->device));
+  if (const char* m = std::getenv("MTLGPU_SWEEP_BLOCKS_PER_SM")) ctx->sweep_blocks_per_sm = std::atoi(m);
   MTLGPU_TRY(dalloc(ctx, &ctx->d_partials, (size_t)kMaxPartials * kPartialWidth));
   MTLGPU_TRY(dalloc(ctx, &ctx->d_counters, kNumCounters));
   MTLGPU_TRY(dalloc(ctx, &ctx->d_scalars, 64));
@@ -84,6 +86,7 @@ void csr_release(Csr* A) {
   dfree(ctx, A->d_v32);
   dfree(ctx, A->d_diag);
   dfree(ctx, A->d_bin_rows);
+  dfree(ctx, A->d_blk);
   dfree(ctx, A->d_trp);
   dfree(ctx, A->d_tci);
   dfree(ctx, A->d_tv);
@@ -408,6 +411,15 @@ mtlgpu_status mtlgpu_pc_sweep(mtlgpu_pc* P, int which, const double* in, double*
   return take_device_error(P->A->ctx);
 }
 
+mtlgpu_status mtlgpu_pc_sweep_f32(mtlgpu_pc* P, int which, const float* in, float* out) {
+  if (!P || (P->kind != MTLGPU_PC_IC0 && P->kind != MTLGPU_PC_ILU0) || in == out ||
+      P->prec != MTLGPU_FP32)
+    return MTLGPU_INVALID_ARG;
+  const SweepPlan& S = which == MTLGPU_LOWER ? P->lower : P->upper;
+  MTLGPU_TRY(sweep_launch<float>(P->A->ctx, S, in, out, false, nullptr));
+  return take_device_error(P->A->ctx);
+}
+
 mtlgpu_status mtlgpu_pc_factor_info(const mtlgpu_pc* P, int which, int* nnz, int* n_levels) {
   if (!P || (P->kind != MTLGPU_PC_IC0 && P->kind != MTLGPU_PC_ILU0)) return MTLGPU_INVALID_ARG;
   if (nnz) *nnz = which == MTLGPU_LOWER ? P->nnz_L : P->nnz_U;
@@ -468,8 +480,10 @@ mtlgpu_status mtlgpu_solve(int method, mtlgpu_csr* A, mtlgpu_pc* P, double* x, c
   if (!A || !prm || !res || (A->n_rows && (!x || !b)) || prm->max_iter < 0)
     return MTLGPU_INVALID_ARG;
   MTLGPU_TRY(set_device(A->ctx));
+  const long long launches_before = A->ctx->launches;
   mtlgpu_status s = solve_impl(method, A, P, x, b, prm, res);
   res->status = s;
+  res->kernel_launches = A->ctx->launches - launches_before;
   return s;
 }
 

@@ -33,6 +33,11 @@ struct Ctx {
   double* d_scalars = nullptr;    // 64 scalar result slots
   double* h_scalars = nullptr;    // pinned mirror (64)
   int* d_error = nullptr;         // device error word: 0 ok, else mtlgpu_status
+  long long launches = 0;         // kernels launched on this context (host-side count)
+  // Resident CTAs per SM for the triangular sweeps (fewer pollers contend
+  // less for L2; 2 measured best on B200).  Benchmark override:
+  // MTLGPU_SWEEP_BLOCKS_PER_SM.
+  int sweep_blocks_per_sm = 2;
 };
 
 // Row-binned SpMV plan: rows grouped by length, each bin processed by a
@@ -67,6 +72,11 @@ struct Csr {
   int32_t* d_bin_rows = nullptr;   // rows ordered by bin (when !uniform)
   std::vector<SpmvBin> bins;
   int tuned_rows_per_group = 1;    // autotuner choice (1 or 2 rows per pass)
+  // CSR-stream row blocks: block b = rows [blk[b], blk[b+1]), <= 32 rows and
+  // <= 32*8 entries, or a single longer row
+  int32_t* d_blk = nullptr;
+  int n_blk = 0;
+  int spmv_kernel = 0;             // 0 = CSR-stream (default), 1 = row-binned groups
   // transpose (built on demand for A^T x)
   int32_t* d_trp = nullptr;
   int32_t* d_tci = nullptr;

@@ -370,6 +370,7 @@ struct Workspace {
   double* history = nullptr;
   int hist_cap = 0;
   cudaGraphExec_t exec = nullptr;
+  size_t graph_nodes = 0;      // kernel nodes per graph launch
   ~Workspace() {}
 };
 
@@ -479,16 +480,28 @@ mtlgpu_status build_graph(Workspace<T>* W) {
   Ctx* ctx = W->A->ctx;
   if (W->exec) return MTLGPU_OK;
   cudaGraph_t g = nullptr;
+  const long long launches_before = ctx->launches;  // captured launches do not run now
   MTLGPU_TRY_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   mtlgpu_status s = MTLGPU_OK;
   for (int k = 0; k < kGraphIters && s == MTLGPU_OK; k++)
     s = W->method == MTLGPU_CG ? record_cg_iteration<T>(W) : record_bicgstab_iteration<T>(W);
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->launches = launches_before;
   if (s != MTLGPU_OK) {
     if (g) cudaGraphDestroy(g);
     return s;
   }
   MTLGPU_TRY_CUDA(ctx, e);
+  size_t nodes = 0;
+  MTLGPU_TRY_CUDA(ctx, cudaGraphGetNodes(g, nullptr, &nodes));
+  std::vector<cudaGraphNode_t> nv(nodes);
+  if (nodes) MTLGPU_TRY_CUDA(ctx, cudaGraphGetNodes(g, nv.data(), &nodes));
+  W->graph_nodes = 0;
+  for (auto nd : nv) {
+    cudaGraphNodeType ty;
+    MTLGPU_TRY_CUDA(ctx, cudaGraphNodeGetType(nd, &ty));
+    W->graph_nodes += ty == cudaGraphNodeTypeKernel;
+  }
   e = cudaGraphInstantiate(&W->exec, g, 0);
   cudaGraphDestroy(g);
   MTLGPU_TRY_CUDA(ctx, e);
@@ -601,6 +614,7 @@ mtlgpu_status run_iterations(Workspace<T>* W, const volatile int* h_interrupt, i
     MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
                                          ctx->stream));
     MTLGPU_TRY_CUDA(ctx, cudaGraphLaunch(W->exec, ctx->stream));
+    ctx->launches += (long long)W->graph_nodes;
     MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (err) break;
   }
@@ -650,6 +664,7 @@ mtlgpu_status device_solve(Workspace<T>* W, const mtlgpu_iter_params* prm, doubl
                                        ctx->stream));
   const int grid = vec_grid(ctx, n);
   if (rhs_is_residual) {
+    ctx->launches++;
     f32_norm_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, reinterpret_cast<const float*>(W->r),
                                                       W->st, ctx->d_partials,
                                                       counter_slot(ctx, 7));
@@ -664,9 +679,11 @@ mtlgpu_status device_solve(Workspace<T>* W, const mtlgpu_iter_params* prm, doubl
     MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->rt, W->r, sizeof(T) * n, cudaMemcpyDeviceToDevice,
                                          ctx->stream));
   init_check_kernel<<<1, 32, 0, ctx->stream>>>(W->st, ident && W->method == MTLGPU_CG);
+  ctx->launches++;
   if (sw) {
     T* second = W->method == MTLGPU_CG ? W->z : W->phat;
     fill2_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, pc_tmp<T>(W->P), second);
+    ctx->launches++;
   }
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   int interrupted = 0;
@@ -777,6 +794,7 @@ static mtlgpu_status solve_mixed(int method, Csr* A, Pc* P, double* d_x, const d
     }
     // inner: A d = r / ||r|| in FP32 from d = 0
     scale_to_f32_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, W64->r, 1.0 / resid, W32->r, W32->x);
+    ctx->launches++;
     MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
     mtlgpu_iter_params ip = *prm;
     ip.rtol = inner_rtol;
@@ -792,6 +810,7 @@ static mtlgpu_status solve_mixed(int method, Csr* A, Pc* P, double* d_x, const d
       if (st != MTLGPU_BREAKDOWN) break;
     }
     refine_update_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, W64->x, W32->x, resid);
+    ctx->launches++;
     MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
     if (st == MTLGPU_BREAKDOWN) break;
   }

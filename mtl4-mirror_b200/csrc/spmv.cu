@@ -27,6 +27,12 @@ using namespace dev;
 namespace {
 
 constexpr int kBlock = 256;
+constexpr int kStreamK = 8;  // entries per lane per row block (CSR-stream)
+
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 
 __device__ __forceinline__ int pow2_group(int len) {
   int g = 2;
@@ -196,6 +202,64 @@ __global__ void __launch_bounds__(kBlock) spmv_cta(int nrows, const int32_t* __r
   finish_epilogue(ep, acc);
 }
 
+// CSR-stream: one warp per row block (<= 32 rows, <= 32*K entries).  Lane l
+// loads entries e0 + l + 32k (k < K): K independent coalesced loads of values
+// and indices, then K gathers of x, all in flight at once; the products are
+// staged in shared memory and lane l sums row r0 + l in column order.  The
+// products and the running sum round separately (no FMA), so every row sum
+// equals the reference's `tmp += A.data[j] * v[A.ref_minor()[j]]`
+// (mat_vec_mult.hpp:666-688) bit for bit.  A block holding a single row
+// longer than 32*K entries is summed by the whole warp instead.
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock)
+    spmv_stream(int n_blocks, const int32_t* __restrict__ blk, const int32_t* __restrict__ rp,
+                const int32_t* __restrict__ ci, const T* __restrict__ val,
+                const T* __restrict__ x, T* __restrict__ y, EpiParams<T> ep) {
+  if (ep.skip && *ep.skip) return;
+  typedef typename AccOf<T, 1>::type R;
+  __shared__ T prod[kBlock / 32][32 * K];
+  R acc = R::zero();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  T* pw = prod[wib];
+  const int warp = (blockIdx.x * kBlock + threadIdx.x) >> 5;
+  const int W = (gridDim.x * kBlock) >> 5;
+  for (int b = warp; b < n_blocks; b += W) {
+    const int r0 = blk[b], r1 = blk[b + 1];
+    const int e0 = rp[r0], e1 = rp[r1];
+    if (e1 - e0 > 32 * K) {  // a single long row
+      T s = T(0);
+      for (int j = e0 + lane; j < e1; j += 32) s = s + val[j] * __ldg(x + ci[j]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+      if (lane == 0) row_epilogue(ep, r0, s, y, acc);
+      continue;
+    }
+    T v[K];
+    int c[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int j = e0 + k * 32 + lane;
+      c[k] = j < e1 ? ci[j] : 0;
+      v[k] = j < e1 ? val[j] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int j = e0 + k * 32 + lane;
+      if (j < e1) pw[k * 32 + lane] = mul_rn(v[k], __ldg(x + c[k]));
+    }
+    __syncwarp();
+    if (lane < r1 - r0) {
+      const int row = r0 + lane;
+      const int b0 = rp[row] - e0, b1 = rp[row + 1] - e0;
+      T s = T(0);
+      for (int j = b0; j < b1; j++) s = add_rn(s, pw[j]);
+      row_epilogue(ep, row, s, y, acc);
+    }
+    __syncwarp();
+  }
+  finish_epilogue(ep, acc);
+}
+
 template <typename T>
 void launch_group(int G, int grid, cudaStream_t st, int nrows, const int32_t* rows,
                   const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y,
@@ -242,6 +306,37 @@ mtlgpu_status csr_analyse(Csr* A) {
   MTLGPU_TRY(take_device_error(ctx));
   A->max_row = (int)h_stats[0];
   A->mean_row = A->n_rows ? double(h_stats[1]) / A->n_rows : 0.0;
+
+  // CSR-stream row blocks (greedy: up to 32 rows and 32*kStreamK entries; a
+  // longer row forms a block of its own)
+  {
+    std::vector<int32_t> h_rp(A->n_rows + 1);
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h_rp.data(), A->d_rp, sizeof(int32_t) * (A->n_rows + 1),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<int32_t> blk;
+    blk.reserve(A->n_rows / 16 + 2);
+    int r = 0;
+    const int cap = 32 * kStreamK;
+    while (r < A->n_rows) {
+      blk.push_back(r);
+      int rows = 0, cnt = 0;
+      while (r < A->n_rows && rows < 32) {
+        const int len = h_rp[r + 1] - h_rp[r];
+        if (rows > 0 && cnt + len > cap) break;
+        cnt += len;
+        rows++;
+        r++;
+        if (cnt > cap) break;
+      }
+    }
+    blk.push_back(A->n_rows);
+    A->n_blk = (int)blk.size() - 1;
+    MTLGPU_TRY(dalloc(ctx, &A->d_blk, blk.size()));
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(A->d_blk, blk.data(), sizeof(int32_t) * blk.size(),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
 
   int g = 2;
   while (g < A->mean_row && g < 32) g <<= 1;
@@ -328,14 +423,24 @@ mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args) {
   ep.skip = args.skip;
   ep.partials = ctx->d_partials;
   ep.counter = counter_slot(ctx, 0);
-  const int rpg = std::max(1, A->tuned_rows_per_group);
-  (void)rpg;
+  if (A->spmv_kernel == 0) {
+    int grid = grid_for(ctx, kBlock / 32, A->n_blk);
+    ep.part_off = 0;
+    ep.part_total = grid;
+    ep.final_launch = true;
+    spmv_stream<T, kStreamK><<<grid, kBlock, 0, ctx->stream>>>(A->n_blk, A->d_blk, A->d_rp,
+                                                              A->d_ci, v, x, y, ep);
+    ctx->launches++;
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    return MTLGPU_OK;
+  }
   if (A->uniform) {
     const int G = A->uniform_group;
     int grid = grid_for(ctx, kBlock / G, A->n_rows);
     ep.part_off = 0;
     ep.part_total = grid;
     ep.final_launch = true;
+    ctx->launches++;
     launch_group<T>(G, grid, ctx->stream, A->n_rows, nullptr, A->d_rp, A->d_ci, v, x, y, ep);
     MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
     return MTLGPU_OK;
@@ -356,6 +461,7 @@ mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args) {
     ep.part_off = off;
     ep.part_total = total;
     ep.final_launch = (k + 1 == A->bins.size());
+    ctx->launches++;
     launch_group<T>(bn.group, grids[k], ctx->stream, bn.count, A->d_bin_rows + bn.begin, A->d_rp,
                     A->d_ci, v, x, y, ep);
     MTLGPU_TRY_CUDA(ctx, cudaGetLastError());

@@ -102,10 +102,19 @@ mtlgpu_status sweep_launch(Ctx* ctx, const SweepPlan& P, const T* in, T* out, bo
   const T* val = PlanVals<T>::val(P);
   const T* dinv = PlanVals<T>::dinv(P);
   if ((P.nnz_off > 0 && !val) || (!P.unit_diag && !dinv)) return MTLGPU_INVALID_ARG;
-  if (!prefilled) MTLGPU_TRY(fill_sentinel<T>(ctx, out, P.n));
+  if (!prefilled) {
+    MTLGPU_TRY(fill_sentinel<T>(ctx, out, P.n));
+    ctx->launches++;
+  }
+  ctx->launches++;
   const int R = 32 / P.group;
   long long warps_needed = (P.n_tasks + 0ll);
+  // Fewer resident warps mean fewer concurrent pollers: with 2 CTAs per SM a
+  // sweep of the 128^3 Laplacian ran 0.53 ms (FP64) against 0.70 ms with 8.
   long long max_warps = (long long)ctx->num_sms * (2048 / 32);
+  if (ctx->sweep_blocks_per_sm > 0)
+    max_warps = std::min(max_warps,
+                         (long long)ctx->num_sms * ctx->sweep_blocks_per_sm * (kBlock / 32));
   long long warps = std::max(1ll, std::min(warps_needed, max_warps));
   int grid = (int)((warps * 32 + kBlock - 1) / kBlock);
   unsigned total_warps = (unsigned)(grid * (kBlock / 32));

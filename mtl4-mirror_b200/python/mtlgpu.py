@@ -51,7 +51,8 @@ class IterParams(C.Structure):
 class IterResult(C.Structure):
     _fields_ = [("error", C.c_int), ("status", C.c_int), ("iterations", C.c_int),
                 ("outer_iterations", C.c_int), ("resid", C.c_double), ("norm_r0", C.c_double),
-                ("true_resid", C.c_double), ("history_len", C.c_int)]
+                ("true_resid", C.c_double), ("history_len", C.c_int),
+                ("kernel_launches", C.c_longlong)]
 
 
 _LIB = None
@@ -271,7 +272,10 @@ class Pc:
         check(_lib().mtlgpu_pc_adjoint_apply(self.h, r.ptr, z.ptr), "pc_adjoint_apply")
 
     def sweep(self, which, x, y):
-        check(_lib().mtlgpu_pc_sweep(self.h, which, x.ptr, y.ptr), "pc_sweep")
+        if x.dtype == np.float32:
+            check(_lib().mtlgpu_pc_sweep_f32(self.h, which, x.ptr, y.ptr), "pc_sweep_f32")
+        else:
+            check(_lib().mtlgpu_pc_sweep(self.h, which, x.ptr, y.ptr), "pc_sweep")
 
     def factor_info(self, which):
         nnz, lev = C.c_int(), C.c_int()
@@ -339,6 +343,15 @@ def solve_host(method, A, P, x, b, **kw):
     st = _lib().mtlgpu_solve_host(METHODS.get(method, method), A.h, P.h if P else None, _p(x),
                                   _p(b), C.byref(prm), C.byref(res))
     return st, res, x
+
+
+def solve_host_ptrs(method, A, P, x_ptr, b_ptr, **kw):
+    """mtlgpu_solve_host on raw host pointers (e.g. pinned buffers)."""
+    prm = make_params(**kw)
+    res = IterResult()
+    st = _lib().mtlgpu_solve_host(METHODS.get(method, method), A.h, P.h if P else None,
+                                  _vp(x_ptr), _vp(b_ptr), C.byref(prm), C.byref(res))
+    return st, res
 
 
 # ---------------------------------------------------------------------------
