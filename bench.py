@@ -163,6 +163,30 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def profile_case(case, grid, launches):
+    """Runs one kernel of the path a few times on an N^3 Laplacian (for
+    profiler captures): 'spmv' (FP64 y = A x), 'sweep64' / 'sweep32' (IC(0)
+    lower sweep in FP64 / FP32)."""
+    import mtlgpu as M
+    A = M.laplacian3d(grid)
+    n = A[0]
+    ctx = M.Context(0)
+    dA = M.Csr(ctx, *A[1:])
+    if case == "spmv":
+        dx, dy = ctx.to_device(M.uniform(n, 5)), ctx.array(n)
+        for _ in range(launches):
+            dA.spmv(dx, dy)
+    else:
+        prec = M.FP32 if case == "sweep32" else M.FP64
+        dt = np.float32 if prec == M.FP32 else np.float64
+        P = M.Pc(dA, "ic0", prec)
+        r, z = ctx.to_device(np.ones(n, dt)), ctx.array(n, dt)
+        for _ in range(launches):
+            P.sweep(M.LOWER, r, z)
+    ctx.synchronize()
+    print(json.dumps({"profile_case": case, "grid": grid, "launches": launches}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -170,7 +194,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mtlgpu", choices=["mtlgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["spmv", "sweep64", "sweep32"])
+    ap.add_argument("--grid", type=int, default=64)
+    ap.add_argument("--launches", type=int, default=3)
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case, args.grid, args.launches)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
