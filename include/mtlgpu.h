@@ -193,6 +193,24 @@ mtlgpu_status mtlgpu_dot(mtlgpu_ctx* ctx, int n, const double* d_x, const double
                          double* h_result);
 mtlgpu_status mtlgpu_two_norm(mtlgpu_ctx* ctx, int n, const double* d_x, double* h_result);
 mtlgpu_status mtlgpu_unary_dot(mtlgpu_ctx* ctx, int n, const double* d_x, double* h_result);
+/* Dot product that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory -- code whose device heap
+ * belongs to a host application or another runtime, or a loop that must not
+ * touch the allocator -- and so cannot create the context mtlgpu_dot needs.
+ * *d_result (a DEVICE pointer) receives x . y for the n-element device
+ * vectors d_x, d_y, computed on `stream` (a cudaStream_t; NULL = the default
+ * stream) of the current device with the same kernel and the same bits as
+ * mtlgpu_dot.  Nothing is allocated: the reduction scratch is a fixed
+ * 32 KiB + 256 B array inside the library that every GPU loading it keeps
+ * until the process exits, holding at most 4096 partial sums; a call needing
+ * more (never on a B200) returns MTLGPU_INCOMPATIBLE_SIZE.
+ * The first call on a device looks up that device's copy of the array (set-up
+ * done once per device); make that first call before any stream capture.
+ * All calls on a device share the array, so calls whose kernels overlap on
+ * the GPU race and give wrong results: order them (one stream, or events). */
+mtlgpu_status mtlgpu_dot_noalloc(int n, const double* d_x, const double* d_y, double* d_result,
+                                 void* stream);
 /* y += alpha * x */
 mtlgpu_status mtlgpu_axpy(mtlgpu_ctx* ctx, int n, double alpha, const double* d_x, double* d_y);
 /* y = x + beta * y */

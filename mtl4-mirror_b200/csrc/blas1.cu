@@ -7,6 +7,7 @@
 // block partials summed by the last block to finish in a fixed order), so
 // repeated calls on the same data give the same bits.
 #include <algorithm>
+#include <mutex>
 
 #include "device.cuh"
 #include "internal.h"
@@ -92,3 +93,104 @@ mtlgpu_status axpby_launch(Ctx* ctx, int n, double alpha, const double* x, doubl
 }
 
 }  // namespace mtlgpu
+
+// ---------------------------------------------------------------------------
+// Dot product for callers that cannot allocate device memory.
+//
+// Some callers cannot call cudaMalloc at all: code running where the device
+// heap belongs to someone else (a host application's own pool, a plugin
+// inside another runtime), or a loop that must not touch the allocator.
+// mtlgpu_dot needs a context, and creating one allocates the reduction
+// scratch.  mtlgpu_dot_noalloc runs the same kernel (dot_kernel, same grid,
+// same reduction order, hence the same bits) with its scratch -- the block
+// partial sums and the arrival counter -- in the file-scope array below, so
+// the call allocates nothing.
+//
+// The array is a fixed 32 KiB + 256 B that every GPU loading this library
+// keeps until the process exits.  It holds at most kNoAllocPartials partial
+// sums; a call whose grid (min(ceil(n / 512), 8 * SM count)) would need more
+// is rejected with MTLGPU_INCOMPATIBLE_SIZE (never the case on a B200, whose
+// grid is at most 1184).  All calls on a device share the array: calls whose
+// kernels overlap on the GPU (different streams, or different host threads
+// without ordering) race on it and give wrong results.  The first call on each
+// device does that device's set-up (cudaGetSymbolAddress of the array, with the
+// device current); that first call should come before any stream capture.
+namespace {
+constexpr int kNoAllocPartials = 4096;
+constexpr size_t kNoAllocCounterOffset = kNoAllocPartials * sizeof(double);
+}  // namespace
+
+// partials[0 .. kNoAllocPartials) | arrival counter (unsigned)
+static __device__ __align__(256) unsigned char g_dot_noalloc_scratch[kNoAllocCounterOffset + 256];
+
+namespace {
+// Per-device set-up: the device address of the array (in host code its name
+// is only a stand-in, never a device address) and the SM count.
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;
+  int num_sms = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+mtlgpu_status noalloc_setup(int device, NoAllocDevice** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return MTLGPU_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoAllocDevice& d = g_noalloc_dev[device];
+  if (!d.ready) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_dot_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return MTLGPU_CUDA_ERROR;
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        sms <= 0) {
+      cudaGetLastError();
+      return MTLGPU_CUDA_ERROR;
+    }
+    d.scratch = static_cast<unsigned char*>(p);
+    d.num_sms = sms;
+    d.ready = true;
+  }
+  *out = &d;
+  return MTLGPU_OK;
+}
+}  // namespace
+
+extern "C" mtlgpu_status mtlgpu_dot_noalloc(int n, const double* d_x, const double* d_y,
+                                            double* d_result, void* stream) {
+  using namespace mtlgpu;
+  if (n < 0 || !d_result || (n > 0 && (!d_x || !d_y))) return MTLGPU_INVALID_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) {
+    cudaGetLastError();
+    return MTLGPU_CUDA_ERROR;
+  }
+  NoAllocDevice* d = nullptr;
+  mtlgpu_status s = noalloc_setup(device, &d);
+  if (s != MTLGPU_OK) return s;
+  if (n == 0) {
+    if (cudaMemsetAsync(d_result, 0, sizeof(double), st) != cudaSuccess) {
+      cudaGetLastError();
+      return MTLGPU_CUDA_ERROR;
+    }
+    return MTLGPU_OK;
+  }
+  // the grid mtlgpu_dot uses on this device
+  const long long need = ((long long)n + 2 * kBlock - 1) / (2 * kBlock);
+  const long long grid = std::max(1ll, std::min(need, (long long)d->num_sms * 8));
+  if (grid > kNoAllocPartials) return MTLGPU_INCOMPATIBLE_SIZE;
+  unsigned* counter = reinterpret_cast<unsigned*>(d->scratch + kNoAllocCounterOffset);
+  // the counter must start at zero (the array keeps the last call's contents)
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned), st) != cudaSuccess) {
+    cudaGetLastError();
+    return MTLGPU_CUDA_ERROR;
+  }
+  dot_kernel<<<(int)grid, kBlock, 0, st>>>(n, d_x, d_y, d_result, d->scratch, counter);
+  if (cudaGetLastError() != cudaSuccess) return MTLGPU_CUDA_ERROR;
+  return MTLGPU_OK;
+}
