@@ -134,8 +134,16 @@ __global__ void transpose_gather_kernel(long long nnz, const int32_t* __restrict
   }
 }
 
-__global__ void d2f_kernel(long long n, const double* __restrict__ a, float* __restrict__ b) {
-  for (long long i = gtid(); i < n; i += gstride()) b[i] = (float)a[i];
+// b = (float)a, and a rounded in place to the same value: factors stored as
+// float are used with float64 vectors at their float values, as
+// ic_0<M, float> / ilu_0<M, float> do (float entries promoted to double inside
+// the trisolves, mtl/operation/lower_trisolve.hpp:173-209).
+__global__ void d2f_kernel(long long n, double* __restrict__ a, float* __restrict__ b) {
+  for (long long i = gtid(); i < n; i += gstride()) {
+    const float f = (float)a[i];
+    b[i] = f;
+    a[i] = (double)f;
+  }
 }
 
 }  // namespace

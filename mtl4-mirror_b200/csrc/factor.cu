@@ -49,7 +49,8 @@ __global__ void jacobi_kernel(int n, const int32_t* __restrict__ diag,
     const int d = diag[i];
     const double a = d >= 0 ? v[d] : 0.0;  // A[i][i] reads 0 where not stored
     const double r = __ddiv_rn(1.0, a);
-    inv[i] = r;
+    // float storage (diagonal<M, float>): both copies hold the float value
+    inv[i] = inv32 ? (double)(float)r : r;
     if (inv32) inv32[i] = (float)r;
   }
 }
