@@ -202,6 +202,7 @@ mtlgpu_status compute_levels(Ctx* ctx, int n, const int32_t* d_rp, const int32_t
 }
 
 void free_sweep_plan(Ctx* ctx, SweepPlan* p) {
+  part_plan_free(ctx, p);
   dfree(ctx, p->d_rp);
   dfree(ctx, p->d_ci);
   dfree(ctx, p->d_val);

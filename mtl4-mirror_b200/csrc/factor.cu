@@ -487,6 +487,9 @@ mtlgpu_status pc_build(Pc* P) {
     MTLGPU_TRY(sweep_plan_make_fp32(ctx, &P->upper));
     MTLGPU_TRY(dalloc(ctx, &P->d_tmp32, n));
   }
+  MTLGPU_TRY(take_device_error(ctx));
+  MTLGPU_TRY(part_plan_build(ctx, &P->lower, P->prec == MTLGPU_FP32));
+  MTLGPU_TRY(part_plan_build(ctx, &P->upper, P->prec == MTLGPU_FP32));
   return take_device_error(ctx);
 }
 
@@ -519,6 +522,9 @@ mtlgpu_status pc_ensure_adjoint(Pc* P) {
     MTLGPU_TRY(sweep_plan_make_fp32(ctx, &P->adj_lower));
     MTLGPU_TRY(sweep_plan_make_fp32(ctx, &P->adj_upper));
   }
+  MTLGPU_TRY(take_device_error(ctx));
+  MTLGPU_TRY(part_plan_build(ctx, &P->adj_lower, P->prec == MTLGPU_FP32));
+  MTLGPU_TRY(part_plan_build(ctx, &P->adj_upper, P->prec == MTLGPU_FP32));
   P->adj_built = true;
   return take_device_error(ctx);
 }

@@ -38,6 +38,10 @@ struct Ctx {
   // less for L2; 2 measured best on B200).  Benchmark override:
   // MTLGPU_SWEEP_BLOCKS_PER_SM.
   int sweep_blocks_per_sm = 2;
+  // Partitioned sweeps (part_sweep.cu): built at preconditioner creation when
+  // enabled (MTLGPU_SWEEP=part|ticket), rows per part (MTLGPU_PART_ROWS).
+  bool part_sweeps = false;
+  int part_rows = 16384;
 };
 
 // Row-binned SpMV plan: rows grouped by length, each bin processed by a
@@ -83,6 +87,21 @@ struct Csr {
   double* d_tv = nullptr;
 };
 
+// Partitioned form of a sweep (part_sweep.cu): rows split into P parts, one
+// CTA each; per precision (0: double, 1: float) a stream of block records.
+struct PartPlan {
+  int P = 0;
+  int max_rows = 0;
+  long long ext_entries = 0;         // entries read from another part
+  struct Prec {
+    bool ready = false;
+    int vals_bytes = 0, offs_bytes = 0, slot_bytes = 0, smem_bytes = 0, n_blocks = 0;
+    int32_t* d_part_blk = nullptr;   // P+1: block range of each part
+    int32_t* d_blk_off16 = nullptr;  // n_blocks+1: record offsets in 16-byte units
+    unsigned char* d_rec = nullptr;  // record stream
+  } prec[2];
+};
+
 // One triangular sweep, stored in processing (level) order.
 // Row t of the plan is original row row_of[t]; its off-diagonal entries are
 // ci/val[rp[t] .. rp[t+1]); dinv[t] is its (inverted) diagonal, absent for a
@@ -104,6 +123,7 @@ struct SweepPlan {
   int32_t* d_level_ptr = nullptr;  // plan rows of each level
   int32_t* d_level = nullptr;      // level of each ORIGINAL row
   unsigned* d_ticket = nullptr;    // [0] = task ticket, [1] = finished warps
+  PartPlan* part = nullptr;        // partitioned form, when built and fitting
 };
 
 struct Pc {
@@ -185,6 +205,18 @@ mtlgpu_status sweep_launch(Ctx* ctx, const SweepPlan& P, const T* in, T* out, bo
                            const int* skip);
 template <typename T>
 mtlgpu_status fill_sentinel(Ctx* ctx, T* p, int n);
+
+// Partitioned sweeps (part_sweep.cu).  part_plan_build runs outside stream
+// capture; without a usable plan (disabled, or a part that does not fit
+// shared memory) S->part stays null and sweeps use sweep_kernel.
+mtlgpu_status part_plan_build(Ctx* ctx, SweepPlan* S, bool with_fp32);
+void part_plan_free(Ctx* ctx, SweepPlan* S);
+void part_plan_free_one(Ctx* ctx, PartPlan* PP, int prec);
+template <typename T>
+bool part_sweep_ready(const SweepPlan& S);
+template <typename T>
+mtlgpu_status part_sweep_launch(Ctx* ctx, const SweepPlan& S, const T* in, T* out,
+                                const int* skip);
 
 // Analysis (analysis.cu)
 mtlgpu_status build_sweep_plan(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_ci,
