@@ -213,7 +213,7 @@ mtlgpu_status part_plan_build(Ctx* ctx, SweepPlan* S, bool with_fp32);
 void part_plan_free(Ctx* ctx, SweepPlan* S);
 void part_plan_free_one(Ctx* ctx, PartPlan* PP, int prec);
 template <typename T>
-bool part_sweep_ready(const SweepPlan& S);
+bool part_sweep_ready(const SweepPlan& S, const T* out);
 template <typename T>
 mtlgpu_status part_sweep_launch(Ctx* ctx, const SweepPlan& S, const T* in, T* out,
                                 const int* skip);

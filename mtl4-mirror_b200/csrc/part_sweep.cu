@@ -18,8 +18,10 @@
 //      farthest dependency one level below it (for a grid in natural order
 //      that is the pencil along the slowest index), if that chain still ends
 //      there;
-//   2. parts: recursive bisection of the chain adjacency graph by BFS
-//      distance from a pseudo-peripheral chain, balanced by row count.
+//   2. parts: two topological orders of the chain dependency graph cut
+//      into strips and tiles, balanced by row count, so that dependencies
+//      between parts all point forward (no two parts wait on each other in
+//      turn).
 // A part's CTA processes its rows level by level.  Values of its own rows
 // live in shared memory (one __syncthreads per block of a level); a
 // dependency on another part is read from the NaN-boxed output vector in
@@ -39,6 +41,7 @@
 // CTA per SM, and a CTA only waits for rows of lower levels, which their CTAs
 // reach without waiting on it; every wait is bounded (MTLGPU_TIMEOUT).
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -53,29 +56,63 @@ using namespace dev;
 namespace {
 
 constexpr int kPartThreads = 256;
-constexpr int kRing = 8;   // record slots in flight
-constexpr int kAhead = 3;  // gathers issued this many blocks ahead
-static_assert(kRing >= 2 * kAhead + 1, "a gather needs its record landed");
+// Ring depth per value type: kRing record slots in flight, gathers issued
+// kAhead blocks ahead (a gather needs its record landed: kRing >= 2 kAhead).
+// FP64 values take more shared memory, which leaves room for fewer slots.
+template <typename T> struct Ring;
+template <> struct Ring<double> { static constexpr int kRing = 10, kAhead = 5; };
+template <> struct Ring<float> { static constexpr int kRing = 16, kAhead = 7; };
+static_assert(Ring<double>::kRing >= 2 * Ring<double>::kAhead, "ring too shallow");
+static_assert(Ring<float>::kRing >= 2 * Ring<float>::kAhead, "ring too shallow");
+constexpr int kRegEnt = 4;  // entries per row held in registers (more: read from the slot)
 
+// Block record: a 48-byte header, then structure-of-arrays sections whose
+// byte offsets the header holds (0: absent), all 16-byte aligned:
+//   out[nrows]        natural index of each row (right-hand side and result)
+//   ref[K][nrows]     first K entries of each row: >= 0 slot of a value of
+//                     this part; kNoEntry: padding; else -(1 + 4 e + lane):
+//                     lane of the e-th gathered 16-byte chunk of `out`
+//   val[K][nrows]     their values
+//   dia[nrows]        inverted diagonal (absent for a unit diagonal)
+//   over[nrows]       entries beyond K: (start << 8) | count in the lists
+//   over_ref[nover], over_val[nover]
+//   gext[next]        natural index of each external value
+// A slot holds the record and then its gather area: rhs[nrows] (element
+// size) and next 16-byte chunks.
 struct RecHdr {
-  int nrows, nent, ngather, slot0;
+  int nrows, next, nover, slot0;
+  int off_ref, off_val, off_dia, off_over;
+  int off_gext, bytes, K, pad;
 };
+static_assert(sizeof(RecHdr) == 48, "record header is three 16-byte words");
+constexpr int kNoEntry = INT32_MIN;
 
 __host__ __device__ __forceinline__ int a16(int b) { return (b + 15) & ~15; }
 
-// Section offsets of a block record (identical on host and device).
-struct RecLayout {
-  int row_beg, gsrc, ref, val, dinv, bytes;
-  __host__ __device__ RecLayout(const RecHdr& h, int tsize, bool unit) {
-    row_beg = 16;
-    gsrc = row_beg + a16(4 * (h.nrows + 1));
-    ref = gsrc + a16(4 * h.ngather);
-    val = ref + a16(4 * h.nent);
-    dinv = val + a16(tsize * h.nent);
-    bytes = dinv + (unit ? 0 : a16(tsize * h.nrows));
-  }
-};
+// Fills the section offsets of h from its counts.
+__host__ __device__ inline void rec_layout(RecHdr& h, int ts, bool unit) {
+  int o = 48 + a16(4 * h.nrows);
+  h.off_ref = o;
+  o += a16(4 * h.K * h.nrows);
+  h.off_val = o;
+  o += a16(ts * h.K * h.nrows);
+  h.off_dia = unit ? 0 : o;
+  if (!unit) o += a16(ts * h.nrows);
+  h.off_over = h.nover ? o : 0;
+  if (h.nover) o += a16(4 * h.nrows) + a16(4 * h.nover) + a16(ts * h.nover);
+  h.off_gext = o;
+  o += a16(4 * h.next);
+  h.bytes = o;
+}
+__host__ __device__ __forceinline__ int slot_need(const RecHdr& h, int ts) {
+  return h.bytes + a16(ts * h.nrows) + 16 * h.next;
+}
 
+template <int N>
+__device__ __forceinline__ void cp_async_ca(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(N) : "memory");
+}
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
@@ -97,8 +134,10 @@ template <typename T>
 __global__ void __launch_bounds__(kPartThreads, 1)
     part_sweep_kernel(const int32_t* __restrict__ part_blk, const int32_t* __restrict__ blk_off16,
                       const unsigned char* __restrict__ recs, int vals_bytes, int offs_bytes,
-                      int slot_bytes, int unit_diag, const T* __restrict__ in, T* out, int* err,
+                      int slot_bytes, const T* __restrict__ in, T* out, int* err,
                       long long limit, const int* skip) {
+  constexpr int kRing = Ring<T>::kRing, kAhead = Ring<T>::kAhead;
+  constexpr int kTs = (int)sizeof(T);
   if (skip && ld_relaxed(skip)) return;
   extern __shared__ __align__(16) unsigned char sm[];
   T* vals = reinterpret_cast<T*>(sm);
@@ -117,16 +156,62 @@ __global__ void __launch_bounds__(kPartThreads, 1)
     unsigned char* dst = slot(k);
     for (int c = tid; c < chunks; c += kPartThreads) cp_async16(dst + 16 * c, src + 16 * c);
   };
+  // right-hand sides at element size (the input is not written during the
+  // sweep), external values as 16-byte chunks through L2
   auto gather = [&](int k) {
     unsigned char* s = slot(k);
+    const RecHdr& h = *reinterpret_cast<const RecHdr*>(s);
+    const int nrows = h.nrows, ng = h.nrows + h.next;
+    const int* orow = reinterpret_cast<const int*>(s + 48);
+    const int* gext = reinterpret_cast<const int*>(s + h.off_gext);
+    unsigned char* g = s + h.bytes;
+    unsigned char* ge = g + a16(kTs * nrows) - 16 * nrows;
+    for (int i = tid; i < ng; i += kPartThreads) {
+      if (i < nrows)
+        cp_async_ca<kTs>(g + kTs * i, in + orow[i]);
+      else
+        cp_async16(ge + 16 * i,
+                   reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(out + gext[i - nrows]) &
+                                                 ~uintptr_t(15)));
+    }
+  };
+
+  // One row of the next block, loaded into registers before its barrier:
+  // after the barrier a row only reads its dependencies' values and runs its
+  // multiply-subtract chain.
+  struct Row {
+    int nrows = 0, slot0 = 0, K = 0, out_idx = 0, over = 0;
+    T rhs = T(0), dia = T(1);
+    int ref[kRegEnt];
+    T val[kRegEnt];
+    T wext[kRegEnt];  // prefetched external value (sentinel: not ready then)
+  };
+  auto load_row = [&](int k, Row& R) {
+    const unsigned char* s = slot(k);
     const RecHdr h = *reinterpret_cast<const RecHdr*>(s);
-    const RecLayout L(h, (int)sizeof(T), unit_diag != 0);
-    const int* gsrc = reinterpret_cast<const int*>(s + L.gsrc);
-    unsigned char* g = s + L.bytes;
-    for (int i = tid; i < h.ngather; i += kPartThreads) {
-      const T* p = (i < h.nrows ? in : out) + gsrc[i];
-      cp_async16(g + 16 * i,
-                 reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(15)));
+    R.nrows = h.nrows;
+    R.slot0 = h.slot0;
+    R.K = h.K;
+    if (tid >= h.nrows) return;
+    R.out_idx = reinterpret_cast<const int*>(s + 48)[tid];
+    R.rhs = reinterpret_cast<const T*>(s + h.bytes)[tid];
+    R.dia = h.off_dia ? reinterpret_cast<const T*>(s + h.off_dia)[tid] : T(1);
+    R.over = h.off_over ? reinterpret_cast<const int*>(s + h.off_over)[tid] : 0;
+    const int* ref = reinterpret_cast<const int*>(s + h.off_ref) + tid;
+    const T* val = reinterpret_cast<const T*>(s + h.off_val) + tid;
+    const unsigned char* ge = s + h.bytes + a16(kTs * h.nrows);
+#pragma unroll
+    for (int q = 0; q < kRegEnt; ++q) {
+      R.ref[q] = kNoEntry;
+      if (q < h.K) {
+        const int r = ref[q * h.nrows];
+        R.ref[q] = r;
+        R.val[q] = val[q * h.nrows];
+        if (r < 0 && r != kNoEntry) {
+          const int code = -r - 1;
+          R.wext[q] = reinterpret_cast<const T*>(ge + 16 * (code >> 2))[code & 3];
+        }
+      }
     }
   };
 
@@ -139,48 +224,61 @@ __global__ void __launch_bounds__(kPartThreads, 1)
     if (k < nb) gather(k);
     cp_async_commit();
   }
+  Row R;
+  cp_async_wait<kAhead - 1>();
+  __syncthreads();
+  if (nb > 0) load_row(0, R);
 
   for (int t = 0; t < nb; ++t) {
-    // Block t's gathers (and, earlier, its record) have landed, and every
-    // thread is done with block t-1, whose slot is refilled next.
-    cp_async_wait<kAhead - 1>();
+    // Block t+1's gathers have landed (and, earlier, its record); the values
+    // of block t-1 are in shared memory; nobody reads block t-1's slot again.
+    cp_async_wait<kAhead - 2>();
     __syncthreads();
+    if (tid < R.nrows) {
+      T w[kRegEnt];
+#pragma unroll
+      for (int q = 0; q < kRegEnt; ++q) w[q] = R.ref[q] >= 0 ? vals[R.ref[q]] : R.wext[q];
+      T rr = R.rhs;
+#pragma unroll
+      for (int q = 0; q < kRegEnt; ++q) {
+        if (R.ref[q] != kNoEntry) {
+          if (R.ref[q] < 0 && Box<T>::is(w[q])) {  // not ready when gathered: poll
+            const RecHdr& h = *reinterpret_cast<const RecHdr*>(slot(t));
+            const int e = (-R.ref[q] - 1) >> 2;
+            w[q] = wait_value(out + reinterpret_cast<const int*>(slot(t) + h.off_gext)[e], limit, err);
+          }
+          rr = sub_rn(rr, mul_rn(R.val[q], w[q]));
+        }
+      }
+      if (R.over) {  // entries beyond K, straight from the slot
+        const unsigned char* s = slot(t);
+        const RecHdr& h = *reinterpret_cast<const RecHdr*>(s);
+        const int* oref = reinterpret_cast<const int*>(s + h.off_over + a16(4 * h.nrows));
+        const T* oval = reinterpret_cast<const T*>(s + h.off_over + a16(4 * h.nrows) + a16(4 * h.nover));
+        const int* gext = reinterpret_cast<const int*>(s + h.off_gext);
+        const unsigned char* ge = s + h.bytes + a16(kTs * h.nrows);
+        const int e0 = R.over >> 8, e1 = e0 + (R.over & 255);
+        for (int e = e0; e < e1; ++e) {
+          const int r = oref[e];
+          T wv;
+          if (r >= 0) {
+            wv = vals[r];
+          } else {
+            const int code = -r - 1;
+            wv = reinterpret_cast<const T*>(ge + 16 * (code >> 2))[code & 3];
+            if (Box<T>::is(wv)) wv = wait_value(out + gext[code >> 2], limit, err);
+          }
+          rr = sub_rn(rr, mul_rn(oval[e], wv));
+        }
+      }
+      rr = canonical(mul_rn(rr, R.dia));
+      vals[R.slot0 + tid] = rr;
+      st_relaxed(out + R.out_idx, rr);
+    }
     if (t + kRing - 1 < nb) copy_rec(t + kRing - 1);
     if (t + kAhead < nb) gather(t + kAhead);
     cp_async_commit();
-
-    const unsigned char* s = slot(t);
-    const RecHdr h = *reinterpret_cast<const RecHdr*>(s);
-    if (tid < h.nrows) {
-      const RecLayout L(h, (int)sizeof(T), unit_diag != 0);
-      const int* row_beg = reinterpret_cast<const int*>(s + L.row_beg);
-      const int* gsrc = reinterpret_cast<const int*>(s + L.gsrc);
-      const int* ref = reinterpret_cast<const int*>(s + L.ref);
-      const T* val = reinterpret_cast<const T*>(s + L.val);
-      const unsigned char* g = s + L.bytes;
-      auto gathered = [&](int i) -> T {
-        const T* p = (i < h.nrows ? in : out) + gsrc[i];
-        return *reinterpret_cast<const T*>(g + 16 * i + (reinterpret_cast<uintptr_t>(p) & 15));
-      };
-      T rr = gathered(tid);
-      const int e1 = row_beg[tid + 1];
-      for (int e = row_beg[tid]; e < e1; ++e) {
-        const int r = ref[e];
-        T w;
-        if (r >= 0) {
-          w = vals[r];
-        } else {
-          const int gi = -r - 1;
-          w = gathered(gi);
-          if (Box<T>::is(w)) w = wait_value(out + gsrc[gi], limit, err);
-        }
-        rr = sub_rn(rr, mul_rn(val[e], w));
-      }
-      if (!unit_diag) rr = mul_rn(rr, reinterpret_cast<const T*>(s + L.dinv)[tid]);
-      rr = canonical(rr);
-      vals[h.slot0 + tid] = rr;
-      st_relaxed(out + gsrc[tid], rr);
-    }
+    if (t + 1 < nb) load_row(t + 1, R);
   }
   cp_async_wait<0>();
 }
@@ -193,81 +291,6 @@ int env_int(const char* name, int dflt) {
   return (s && *s) ? std::atoi(s) : dflt;
 }
 
-// Recursive bisection of the chain graph (CSR adj_ptr/adj) into `parts`
-// parts balanced by row count (len); result in part_of[chain].
-struct Bisector {
-  const std::vector<int>& adj_ptr;
-  const std::vector<int>& adj;
-  const std::vector<int>& len;
-  std::vector<int>& part_of;
-  std::vector<int> member, seen;
-  int stamp = 0;
-
-  Bisector(const std::vector<int>& ap, const std::vector<int>& a, const std::vector<int>& l,
-           std::vector<int>& po)
-      : adj_ptr(ap), adj(a), len(l), part_of(po), member(l.size(), -1), seen(l.size(), -1) {}
-
-  // BFS order over the members of set `set_id` from `start`, continuing from
-  // the next unvisited member (in `nodes` order) when a component runs out.
-  void bfs(const std::vector<int>& nodes, int set_id, int start, std::vector<int>& order) {
-    const int vs = ++stamp;
-    order.clear();
-    size_t head = 0, next_unvisited = 0;
-    auto push = [&](int c) {
-      seen[c] = vs;
-      order.push_back(c);
-    };
-    push(start);
-    while (order.size() < nodes.size()) {
-      if (head == order.size()) {
-        while (seen[nodes[next_unvisited]] == vs) ++next_unvisited;
-        push(nodes[next_unvisited]);
-      }
-      const int c = order[head++];
-      for (int k = adj_ptr[c]; k < adj_ptr[c + 1]; ++k) {
-        const int d = adj[k];
-        if (member[d] == set_id && seen[d] != vs) push(d);
-      }
-    }
-  }
-
-  void run(std::vector<int>& nodes, int parts, int first, int& set_counter) {
-    if (parts <= 1 || nodes.size() <= 1) {
-      for (int c : nodes) part_of[c] = first;
-      return;
-    }
-    const int set_id = ++set_counter;
-    for (int c : nodes) member[c] = set_id;
-    std::vector<int> order;
-    // pseudo-peripheral start: BFS sweeps from the first node
-    bfs(nodes, set_id, nodes[0], order);
-    bfs(nodes, set_id, order.back(), order);
-    bfs(nodes, set_id, order.back(), order);
-    long long total = 0;
-    for (int c : nodes) total += len[c];
-    const int p1 = parts / 2;
-    const long long target = total * p1 / parts;
-    std::vector<int> a, b;
-    long long acc = 0;
-    for (int c : order) {
-      if (a.empty() || (b.empty() && acc + len[c] / 2 <= target)) {
-        a.push_back(c);
-        acc += len[c];
-      } else {
-        b.push_back(c);
-      }
-    }
-    if (b.empty()) {
-      b.push_back(a.back());
-      a.pop_back();
-    }
-    std::vector<int>().swap(nodes);
-    std::vector<int>().swap(order);
-    run(a, p1, first, set_counter);
-    run(b, parts - p1, first + p1, set_counter);
-  }
-};
-
 }  // namespace
 
 // Host side of the partitioning: the level-ordered plan in, block records
@@ -279,9 +302,12 @@ struct PartInput {
   const int32_t *lp = nullptr, *row_of = nullptr, *rp = nullptr, *ci = nullptr;
   const double *val = nullptr, *dinv = nullptr;
   int num_sms = 148, rows_per_part = 16384, smem_optin = 232448;
+  // optional: the part of each row (natural index), e.g. from the geometry
+  // the caller knows; parts are then 0 .. max+1 and chains are not formed
+  const int32_t* part_of_row = nullptr;
 };
 struct HostPart {
-  int P = 0, max_rows = 0;
+  int P = 0, max_rows = 0, n_chains = 0;
   long long ext_entries = 0;
   struct Prec {
     int vals_bytes = 0, offs_bytes = 0, slot_bytes = 0, smem_bytes = 0;
@@ -302,86 +328,165 @@ bool part_plan_host(const PartInput& in, HostPart* out) {
   P = std::max(1, P);
   const int max_chain = std::max(1, ((n + P - 1) / P) / 4);
 
-  // 1. chains
-  std::vector<int> chain_of(n), tail, clen;
-  for (int p = 0; p < n; ++p) {
-    const int r = in.row_of[p];
-    int best = -1;
-    long long best_dist = -1;
-    for (int e = in.rp[p]; e < in.rp[p + 1]; ++e) {
-      const int q = pos_of[in.ci[e]];
-      if (lev[q] != lev[p] - 1) continue;
-      const int ch = chain_of[q];
-      if (tail[ch] != q || clen[ch] >= max_chain) continue;
-      const long long dist = std::llabs((long long)in.ci[e] - r);
-      if (dist > best_dist) best_dist = dist, best = ch;
-    }
-    if (best < 0) {
-      best = (int)tail.size();
-      tail.push_back(p);
-      clen.push_back(0);
-    }
-    chain_of[p] = best;
-    tail[best] = p;
-    clen[best]++;
-  }
-  const int nc = (int)tail.size();
-
-  // 2. chain adjacency (unique neighbours, both directions)
-  std::vector<int> cptr(nc + 1, 0), crows(n);
-  for (int p = 0; p < n; ++p) cptr[chain_of[p] + 1]++;
-  for (int c = 0; c < nc; ++c) cptr[c + 1] += cptr[c];
-  {
-    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
-    for (int p = 0; p < n; ++p) crows[fill[chain_of[p]]++] = p;
-  }
-  std::vector<int> mark(nc, -1), out_ptr(nc + 1, 0), out_adj;
-  for (int c = 0; c < nc; ++c) {
-    for (int k = cptr[c]; k < cptr[c + 1]; ++k) {
-      const int p = crows[k];
-      for (int e = in.rp[p]; e < in.rp[p + 1]; ++e) {
-        const int d = chain_of[pos_of[in.ci[e]]];
-        if (d != c && mark[d] != c) {
-          mark[d] = c;
-          out_adj.push_back(d);
+  std::vector<int> part_of(n);
+  if (in.part_of_row) {
+    P = 0;
+    for (int p = 0; p < n; ++p) P = std::max(P, in.part_of_row[in.row_of[p]] + 1);
+    if (P > in.num_sms) return false;
+    for (int p = 0; p < n; ++p) part_of[p] = in.part_of_row[in.row_of[p]];
+  } else {
+    // 1. chains.  Level by level, each row claims the chain ending at one of
+    // its dependencies one level below; claims are granted farthest first
+    // (largest |column - row|), so that on a grid in natural order the
+    // chains are the pencils along the slowest index.
+    std::vector<int> chain_of(n, -1), tail, clen;
+    struct Claim {
+      long long dist;
+      int p, q;
+    };
+    std::vector<Claim> claims;
+    for (int l = 0; l < in.n_levels; ++l) {
+      claims.clear();
+      for (int p = in.lp[l]; p < in.lp[l + 1]; ++p) {
+        const int r = in.row_of[p];
+        for (int e = in.rp[p]; e < in.rp[p + 1]; ++e) {
+          const int q = pos_of[in.ci[e]];
+          if (lev[q] == l - 1) claims.push_back({std::llabs((long long)in.ci[e] - r), p, q});
         }
       }
+      std::stable_sort(claims.begin(), claims.end(),
+                       [](const Claim& a, const Claim& b) { return a.dist > b.dist; });
+      for (const Claim& c : claims) {
+        if (chain_of[c.p] >= 0) continue;
+        const int ch = chain_of[c.q];
+        if (tail[ch] != c.q || clen[ch] >= max_chain) continue;
+        chain_of[c.p] = ch;
+        tail[ch] = c.p;
+        clen[ch]++;
+      }
+      for (int p = in.lp[l]; p < in.lp[l + 1]; ++p) {
+        if (chain_of[p] >= 0) continue;
+        chain_of[p] = (int)tail.size();
+        tail.push_back(p);
+        clen.push_back(1);
+      }
     }
-    out_ptr[c + 1] = (int)out_adj.size();
-  }
-  std::vector<int> in_ptr(nc + 1, 0), in_adj(out_adj.size());
-  for (int d : out_adj) in_ptr[d + 1]++;
-  for (int c = 0; c < nc; ++c) in_ptr[c + 1] += in_ptr[c];
-  {
-    std::vector<int> fill(in_ptr.begin(), in_ptr.end() - 1);
-    for (int c = 0; c < nc; ++c)
-      for (int k = out_ptr[c]; k < out_ptr[c + 1]; ++k) in_adj[fill[out_adj[k]]++] = c;
-  }
-  std::vector<int> adj_ptr(nc + 1, 0), adj;
-  std::fill(mark.begin(), mark.end(), -1);
-  for (int c = 0; c < nc; ++c) {
-    for (int k = out_ptr[c]; k < out_ptr[c + 1]; ++k)
-      if (mark[out_adj[k]] != c) mark[out_adj[k]] = c, adj.push_back(out_adj[k]);
-    for (int k = in_ptr[c]; k < in_ptr[c + 1]; ++k)
-      if (mark[in_adj[k]] != c) mark[in_adj[k]] = c, adj.push_back(in_adj[k]);
-    adj_ptr[c + 1] = (int)adj.size();
-  }
-  std::vector<int>().swap(out_adj);
-  std::vector<int>().swap(in_adj);
+    const int nc = (int)tail.size();
 
-  // 3. parts
-  std::vector<int> part_of_chain(nc, 0);
-  {
-    std::vector<int> nodes(nc);
-    for (int c = 0; c < nc; ++c) nodes[c] = c;
-    Bisector B(adj_ptr, adj, clen, part_of_chain);
-    int sets = 0;
-    B.run(nodes, P, 0, sets);
+    // 2. chain dependency graph: out_adj[c] = chains that c's rows depend on,
+    // in_adj[c] = chains depending on c (unique entries)
+    std::vector<int> cptr(nc + 1, 0), crows(n);
+    for (int p = 0; p < n; ++p) cptr[chain_of[p] + 1]++;
+    for (int c = 0; c < nc; ++c) cptr[c + 1] += cptr[c];
+    {
+      std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+      for (int p = 0; p < n; ++p) crows[fill[chain_of[p]]++] = p;
+    }
+    std::vector<int> mark(nc, -1), out_ptr(nc + 1, 0), out_adj;
+    for (int c = 0; c < nc; ++c) {
+      for (int k = cptr[c]; k < cptr[c + 1]; ++k) {
+        const int p = crows[k];
+        for (int e = in.rp[p]; e < in.rp[p + 1]; ++e) {
+          const int d = chain_of[pos_of[in.ci[e]]];
+          if (d != c && mark[d] != c) {
+            mark[d] = c;
+            out_adj.push_back(d);
+          }
+        }
+      }
+      out_ptr[c + 1] = (int)out_adj.size();
+    }
+    std::vector<int> in_ptr(nc + 1, 0), in_adj(out_adj.size());
+    for (int d : out_adj) in_ptr[d + 1]++;
+    for (int c = 0; c < nc; ++c) in_ptr[c + 1] += in_ptr[c];
+    {
+      std::vector<int> fill(in_ptr.begin(), in_ptr.end() - 1);
+      for (int c = 0; c < nc; ++c)
+        for (int k = out_ptr[c]; k < out_ptr[c + 1]; ++k) in_adj[fill[out_adj[k]]++] = c;
+    }
+
+    // 3. parts.  Two topological orders of the chain dependency graph
+    // (Kahn's algorithm taking, among the ready chains, the one whose first
+    // row has the smallest index -- L1 -- or the largest -- L2; on a grid in
+    // natural order these are the row-major and column-major orders of the
+    // pencils).  sqrt(P) strips are cut along L1 and each strip into tiles
+    // along L2, balanced by row count.  Every dependency then points to the
+    // same or a later part, so neighbouring parts never wait on each other
+    // in turn, and on a grid the tiles are rectangles whose boundaries a
+    // dependency path crosses about 2 sqrt(P) times.
+    std::vector<int> part_of_chain(nc, 0);
+    {
+      std::vector<int> head(nc);
+      for (int p = n - 1; p >= 0; --p) head[chain_of[p]] = in.row_of[p];
+      auto kahn = [&](bool smallest_first) {
+        std::vector<int> rank(nc, -1), indeg(nc);
+        for (int c = 0; c < nc; ++c) indeg[c] = out_ptr[c + 1] - out_ptr[c];
+        auto cmp = [&](int a, int b) {  // heap order: top = next to take
+          return smallest_first ? head[a] > head[b] : head[a] < head[b];
+        };
+        std::vector<int> heap;
+        for (int c = 0; c < nc; ++c)
+          if (indeg[c] == 0) heap.push_back(c);
+        std::make_heap(heap.begin(), heap.end(), cmp);
+        int next = 0, scan = 0;
+        while (next < nc) {
+          if (heap.empty()) {  // a cycle between chains: release the first one left
+            while (rank[scan] >= 0) ++scan;
+            indeg[scan] = 0;
+            heap.push_back(scan);
+          }
+          std::pop_heap(heap.begin(), heap.end(), cmp);
+          const int c = heap.back();
+          heap.pop_back();
+          if (rank[c] >= 0) continue;
+          rank[c] = next++;
+          for (int k = in_ptr[c]; k < in_ptr[c + 1]; ++k) {
+            const int d = in_adj[k];
+            if (rank[d] < 0 && --indeg[d] == 0) {
+              heap.push_back(d);
+              std::push_heap(heap.begin(), heap.end(), cmp);
+            }
+          }
+        }
+        return rank;
+      };
+      const std::vector<int> L1 = kahn(true), L2 = kahn(false);
+      std::vector<int> order(nc);
+      for (int c = 0; c < nc; ++c) order[L1[c]] = c;
+      long long total = 0;
+      for (int c = 0; c < nc; ++c) total += clen[c];
+      const int S = std::max(1, std::min(P, (int)std::lround(std::sqrt((double)P))));
+      size_t pos = 0;
+      int first_part = 0;
+      long long done_rows = 0;
+      for (int st = 0; st < S; ++st) {
+        const int ps = P / S + (st < P % S ? 1 : 0);
+        const long long strip_end = total * (first_part + ps) / P;
+        std::vector<int> strip;
+        while (pos < order.size() &&
+               (strip.empty() || st == S - 1 || done_rows + clen[order[pos]] / 2 <= strip_end)) {
+          strip.push_back(order[pos]);
+          done_rows += clen[order[pos]];
+          ++pos;
+        }
+        std::sort(strip.begin(), strip.end(), [&](int a, int b) { return L2[a] < L2[b]; });
+        long long sw = 0, acc = 0;
+        for (int c : strip) sw += clen[c];
+        int k = 0;
+        for (int c : strip) {
+          while (k < ps - 1 && acc + clen[c] / 2 > sw * (k + 1) / ps) ++k;
+          part_of_chain[c] = first_part + k;
+          acc += clen[c];
+        }
+        first_part += ps;
+      }
+    }
+    for (int p = 0; p < n; ++p) part_of[p] = part_of_chain[chain_of[p]];
+    out->n_chains = nc;
   }
 
   // 4. rows of each part in level order (plan order is level order); slots
-  std::vector<int> part_ptr(P + 1, 0), part_rows(n), slot_of(n), part_of(n);
-  for (int p = 0; p < n; ++p) part_of[p] = part_of_chain[chain_of[p]];
+  std::vector<int> part_ptr(P + 1, 0), part_rows(n), slot_of(n);
   for (int p = 0; p < n; ++p) part_ptr[part_of[p] + 1]++;
   for (int q = 0; q < P; ++q) part_ptr[q + 1] += part_ptr[q];
   {
@@ -399,10 +504,16 @@ bool part_plan_host(const PartInput& in, HostPart* out) {
   out->max_rows = max_rows;
   long long ext_entries = 0;
 
+  // entries per row held in the record's fixed columns
+  int K = 0;
+  for (int p = 0; p < n; ++p) K = std::max(K, in.rp[p + 1] - in.rp[p]);
+  K = std::min(K, kRegEnt);
+
   // 5. block records, per precision.  A slot holds one block's record and,
-  // right after it, the block's gather area (16 bytes per gathered value).
+  // right after it, the block's gather area.
   for (int prec = 0; prec < (in.with_fp32 ? 2 : 1); ++prec) {
     const int ts = prec == 0 ? 8 : 4;
+    const int kRing = prec == 0 ? Ring<double>::kRing : Ring<float>::kRing;
     const int vals_bytes = a16(max_rows * ts);
     int offs_bytes = 8192;
     bool ok = false;
@@ -422,15 +533,22 @@ bool part_plan_host(const PartInput& in, HostPart* out) {
         int nblk = 0;
         for (int i = part_ptr[q], iend = part_ptr[q + 1]; i < iend;) {
           // grow a block from row i: one level, <= kPartThreads rows, fits a slot
-          RecHdr h{0, 0, 0, i - part_ptr[q]};
+          RecHdr h{};
+          h.slot0 = i - part_ptr[q];
+          h.K = K;
           int j = i;
           const int l0 = lev[part_rows[i]];
           while (j < iend && h.nrows < kPartThreads && lev[part_rows[j]] == l0) {
             const int p = part_rows[j];
+            const int ne = in.rp[p + 1] - in.rp[p];
             int ext = 0;
             for (int e = in.rp[p]; e < in.rp[p + 1]; ++e) ext += part_of[pos_of[in.ci[e]]] != q;
-            const RecHdr t{h.nrows + 1, h.nent + in.rp[p + 1] - in.rp[p], h.ngather + 1 + ext, h.slot0};
-            if (RecLayout(t, ts, in.unit_diag).bytes + 16 * t.ngather > slot_bytes) break;
+            RecHdr t = h;
+            t.nrows += 1;
+            t.next += ext;
+            t.nover += std::max(0, ne - K);
+            rec_layout(t, ts, in.unit_diag);
+            if (ne - K > 255 || slot_need(t, ts) > slot_bytes) break;
             h = t;
             ++j;
           }
@@ -438,43 +556,54 @@ bool part_plan_host(const PartInput& in, HostPart* out) {
             fits = false;
             break;
           }
-          const RecLayout L(h, ts, in.unit_diag);
+          rec_layout(h, ts, in.unit_diag);
           const size_t base = stream.size();
-          stream.resize(base + L.bytes, 0);
+          stream.resize(base + h.bytes, 0);
           unsigned char* rec = stream.data() + base;
           std::memcpy(rec, &h, sizeof(h));
-          int32_t* rb = reinterpret_cast<int32_t*>(rec + L.row_beg);
-          int32_t* gs = reinterpret_cast<int32_t*>(rec + L.gsrc);
-          int32_t* rf = reinterpret_cast<int32_t*>(rec + L.ref);
-          // gather list: the rows' own right-hand sides first, then externals
-          int ne = 0, ng = h.nrows;
+          int32_t* orow = reinterpret_cast<int32_t*>(rec + 48);
+          int32_t* rf = reinterpret_cast<int32_t*>(rec + h.off_ref);
+          int32_t* gext = reinterpret_cast<int32_t*>(rec + h.off_gext);
+          int32_t* over = h.off_over ? reinterpret_cast<int32_t*>(rec + h.off_over) : nullptr;
+          int32_t* oref = h.off_over ? over + a16(4 * h.nrows) / 4 : nullptr;
+          unsigned char* oval = h.off_over ? rec + h.off_over + a16(4 * h.nrows) + a16(4 * h.nover)
+                                           : nullptr;
+          auto put_val = [&](unsigned char* base_v, int idx, double v) {
+            if (ts == 8)
+              reinterpret_cast<double*>(base_v)[idx] = v;
+            else
+              reinterpret_cast<float*>(base_v)[idx] = (float)v;
+          };
+          const int lanes = 16 / ts;
+          int ng = 0, no = 0;
           for (int k = 0; k < h.nrows; ++k) {
             const int p = part_rows[i + k];
-            rb[k] = ne;
-            gs[k] = in.row_of[p];
-            for (int e = in.rp[p]; e < in.rp[p + 1]; ++e, ++ne) {
+            orow[k] = in.row_of[p];
+            const int ne = in.rp[p + 1] - in.rp[p];
+            if (over) over[k] = ne > K ? (no << 8) | (ne - K) : 0;
+            for (int q2 = 0; q2 < K; ++q2) rf[q2 * h.nrows + k] = kNoEntry;
+            for (int e = in.rp[p], c = 0; e < in.rp[p + 1]; ++e, ++c) {
               const int qd = pos_of[in.ci[e]];
+              int r;
               if (part_of[qd] == q) {
-                rf[ne] = slot_of[qd];
+                r = slot_of[qd];
               } else {
-                gs[ng] = in.ci[e];
-                rf[ne] = -(ng + 1);
+                gext[ng] = in.ci[e];
+                r = -(1 + 4 * ng + in.ci[e] % lanes);
                 ++ng;
               }
-              if (ts == 8)
-                reinterpret_cast<double*>(rec + L.val)[ne] = in.val[e];
-              else
-                reinterpret_cast<float*>(rec + L.val)[ne] = (float)in.val[e];
+              if (c < K) {
+                rf[c * h.nrows + k] = r;
+                put_val(rec + h.off_val, c * h.nrows + k, in.val[e]);
+              } else {
+                oref[no] = r;
+                put_val(oval, no, in.val[e]);
+                ++no;
+              }
             }
-            if (!in.unit_diag) {
-              if (ts == 8)
-                reinterpret_cast<double*>(rec + L.dinv)[k] = in.dinv[p];
-              else
-                reinterpret_cast<float*>(rec + L.dinv)[k] = (float)in.dinv[p];
-            }
+            if (!in.unit_diag) put_val(rec + h.off_dia, k, in.dinv[p]);
           }
-          rb[h.nrows] = ne;
-          ext_entries += ng - h.nrows;
+          ext_entries += ng;
           blk_off16.push_back((int32_t)(stream.size() / 16));
           ++nblk;
           i = j;
@@ -616,9 +745,12 @@ void part_plan_free(Ctx* ctx, SweepPlan* S) {
   S->part = nullptr;
 }
 
+// External values are read as 16-byte chunks whose lane the records fix, so
+// the output vector must be 16-byte aligned (device allocations are).
 template <typename T>
-bool part_sweep_ready(const SweepPlan& S) {
-  return S.part && S.part->prec[sizeof(T) == 8 ? 0 : 1].ready;
+bool part_sweep_ready(const SweepPlan& S, const T* out) {
+  return S.part && S.part->prec[sizeof(T) == 8 ? 0 : 1].ready &&
+         (reinterpret_cast<uintptr_t>(out) & 15) == 0;
 }
 
 template <typename T>
@@ -627,14 +759,14 @@ mtlgpu_status part_sweep_launch(Ctx* ctx, const SweepPlan& S, const T* in, T* ou
   const auto& V = S.part->prec[sizeof(T) == 8 ? 0 : 1];
   ctx->launches++;
   part_sweep_kernel<T><<<S.part->P, kPartThreads, V.smem_bytes, ctx->stream>>>(
-      V.d_part_blk, V.d_blk_off16, V.d_rec, V.vals_bytes, V.offs_bytes, V.slot_bytes,
-      S.unit_diag ? 1 : 0, in, out, ctx->d_error, ctx->spin_limit, skip);
+      V.d_part_blk, V.d_blk_off16, V.d_rec, V.vals_bytes, V.offs_bytes, V.slot_bytes, in, out,
+      ctx->d_error, ctx->spin_limit, skip);
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
 }
 
-template bool part_sweep_ready<double>(const SweepPlan&);
-template bool part_sweep_ready<float>(const SweepPlan&);
+template bool part_sweep_ready<double>(const SweepPlan&, const double*);
+template bool part_sweep_ready<float>(const SweepPlan&, const float*);
 template mtlgpu_status part_sweep_launch<double>(Ctx*, const SweepPlan&, const double*, double*,
                                                  const int*);
 template mtlgpu_status part_sweep_launch<float>(Ctx*, const SweepPlan&, const float*, float*,

@@ -106,7 +106,7 @@ mtlgpu_status sweep_launch(Ctx* ctx, const SweepPlan& P, const T* in, T* out, bo
     MTLGPU_TRY(fill_sentinel<T>(ctx, out, P.n));
     ctx->launches++;
   }
-  if (part_sweep_ready<T>(P)) return part_sweep_launch<T>(ctx, P, in, out, skip);
+  if (part_sweep_ready<T>(P, out)) return part_sweep_launch<T>(ctx, P, in, out, skip);
   ctx->launches++;
   const int R = 32 / P.group;
   long long warps_needed = (P.n_tasks + 0ll);
