@@ -265,7 +265,7 @@ def main():
         barrier()
         return e0.elapsed_time(e1) / reps, out
 
-    mixed_kw = dict(rtol=1e-10, max_iter=4000, mode=M.SOLVE_MIXED, inner_rtol=1e-4)
+    mixed_kw = dict(rtol=1e-10, max_iter=4000, mode=M.SOLVE_MIXED, inner_rtol=1e-6)
     fp64_kw = dict(rtol=1e-10, max_iter=2000)
 
     def solve_mixed():

@@ -107,7 +107,9 @@ typedef struct {
   double norm_r0;        /* < 0: use two_norm(b), as basic_iteration(b, ...) */
   int mode;              /* mtlgpu_solve_mode */
   /* MIXED_REFINED only: */
-  double inner_rtol;     /* relative reduction asked of each FP32 inner solve (0: 1e-4) */
+  double inner_rtol;     /* largest relative reduction asked of one FP32 inner
+                            solve (0: 1e-6); an inner solve never asks for more
+                            than half the reduction still needed */
   int inner_max_iter;    /* per inner solve (0: max_iter)  */
   int max_outer;         /* refinement steps (0: 30) */
   /* optional: */

@@ -770,7 +770,7 @@ static mtlgpu_status solve_mixed(int method, Csr* A, Pc* P, double* d_x, const d
     norm_r0 = std::sqrt(nb2);
   }
   const double tol = prm->rtol * norm_r0;
-  const double inner_rtol = prm->inner_rtol > 0 ? prm->inner_rtol : 1e-4;
+  const double inner_rtol = prm->inner_rtol > 0 ? prm->inner_rtol : 1e-6;
   const int max_outer = prm->max_outer > 0 ? prm->max_outer : 30;
   const int inner_max = prm->inner_max_iter > 0 ? prm->inner_max_iter : prm->max_iter;
   int total = 0, outer = 0, hist = 0;
@@ -796,8 +796,12 @@ static mtlgpu_status solve_mixed(int method, Csr* A, Pc* P, double* d_x, const d
     scale_to_f32_kernel<<<grid, kBlock, 0, ctx->stream>>>(n, W64->r, 1.0 / resid, W32->r, W32->x);
     ctx->launches++;
     MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    // Each inner solve asks for at most inner_rtol, and never for more than
+    // the reduction still needed (with a margin of 2): the last refinement
+    // step then costs only the iterations it needs.
     mtlgpu_iter_params ip = *prm;
-    ip.rtol = inner_rtol;
+    const double target = std::max(tol, prm->atol);
+    ip.rtol = std::max(inner_rtol, std::min(0.5, 0.5 * target / resid));
     ip.atol = 0;
     int it = 0, ec = 0, st = 0, hl = 0;
     double rr = 0;

@@ -55,13 +55,15 @@ using namespace dev;
 
 namespace {
 
-constexpr int kPartThreads = 256;
+constexpr int kPartThreads = 256;   // consumer threads: rows per block at most
+constexpr int kProducers = 64;      // producer threads (two warps): copies and gathers
+constexpr int kCtaThreads = kPartThreads + kProducers;
 // Ring depth per value type: kRing record slots in flight, gathers issued
 // kAhead blocks ahead (a gather needs its record landed: kRing >= 2 kAhead).
 // FP64 values take more shared memory, which leaves room for fewer slots.
 template <typename T> struct Ring;
 template <> struct Ring<double> { static constexpr int kRing = 10, kAhead = 5; };
-template <> struct Ring<float> { static constexpr int kRing = 16, kAhead = 7; };
+template <> struct Ring<float> { static constexpr int kRing = 16, kAhead = 8; };
 static_assert(Ring<double>::kRing >= 2 * Ring<double>::kAhead, "ring too shallow");
 static_assert(Ring<float>::kRing >= 2 * Ring<float>::kAhead, "ring too shallow");
 constexpr int kRegEnt = 4;  // entries per row held in registers (more: read from the slot)
@@ -125,13 +127,67 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// mbarrier helpers (shared::cta, 64-bit barrier objects).
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b))
+      : "memory");
+}
+// Arrives on b expecting `bytes` of asynchronous copies to complete on it.
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+          smem_u32(b)),
+      "r"(bytes)
+      : "memory");
+}
+// Bulk copy global -> this CTA's shared memory (TMA, no multicast), completing
+// its bytes on mbarrier b.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes,
+                                              unsigned long long* b) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(b))
+      : "memory");
+}
+// Arrives on b once every cp.async this thread issued before has completed.
+__device__ __forceinline__ void mbar_arrive_cp_async(unsigned long long* b) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase with the given parity; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, long long limit) {
+  for (long long k = 0; k < limit; ++k)
+    if (mbar_test(b, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void consumer_sync() {  // the kPartThreads consumer threads only
+  asm volatile("bar.sync 1, %0;" ::"n"(kPartThreads) : "memory");
+}
+
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
 
 template <typename T>
-__global__ void __launch_bounds__(kPartThreads, 1)
+__global__ void __launch_bounds__(kCtaThreads, 1)
     part_sweep_kernel(const int32_t* __restrict__ part_blk, const int32_t* __restrict__ blk_off16,
                       const unsigned char* __restrict__ recs, int vals_bytes, int offs_bytes,
                       int slot_bytes, const T* __restrict__ in, T* out, int* err,
@@ -140,58 +196,91 @@ __global__ void __launch_bounds__(kPartThreads, 1)
   constexpr int kTs = (int)sizeof(T);
   if (skip && ld_relaxed(skip)) return;
   extern __shared__ __align__(16) unsigned char sm[];
+  // Per slot: rec_full (its record copied), full (record and gathers landed),
+  // empty (every consumer warp done with it).
+  __shared__ unsigned long long rec_full[kRing], full[kRing], empty[kRing];
+  __shared__ int abort_flag;
   T* vals = reinterpret_cast<T*>(sm);
   int32_t* offs = reinterpret_cast<int32_t*>(sm + vals_bytes);
   unsigned char* ring = sm + vals_bytes + offs_bytes;
   const int tid = threadIdx.x;
   const int b0 = part_blk[blockIdx.x];
   const int nb = part_blk[blockIdx.x + 1] - b0;
-  for (int i = tid; i <= nb; i += kPartThreads) offs[i] = blk_off16[b0 + i];
+  for (int i = tid; i <= nb; i += kCtaThreads) offs[i] = blk_off16[b0 + i];
+  if (tid < kRing) {
+    mbar_init(&rec_full[tid], 1);
+    mbar_init(&full[tid], kProducers);
+    mbar_init(&empty[tid], kPartThreads / 32);
+    // make the initialised barriers visible to the bulk-copy (async) proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (tid == 0) abort_flag = 0;
   __syncthreads();
-
   auto slot = [&](int k) { return ring + (k % kRing) * slot_bytes; };
-  auto copy_rec = [&](int k) {
-    const unsigned char* src = recs + (size_t)offs[k] * 16;
-    const int chunks = offs[k + 1] - offs[k];
-    unsigned char* dst = slot(k);
-    for (int c = tid; c < chunks; c += kPartThreads) cp_async16(dst + 16 * c, src + 16 * c);
-  };
-  // right-hand sides at element size (the input is not written during the
-  // sweep), external values as 16-byte chunks through L2
-  auto gather = [&](int k) {
-    unsigned char* s = slot(k);
-    const RecHdr& h = *reinterpret_cast<const RecHdr*>(s);
-    const int nrows = h.nrows, ng = h.nrows + h.next;
-    const int* orow = reinterpret_cast<const int*>(s + 48);
-    const int* gext = reinterpret_cast<const int*>(s + h.off_gext);
-    unsigned char* g = s + h.bytes;
-    unsigned char* ge = g + a16(kTs * nrows) - 16 * nrows;
-    for (int i = tid; i < ng; i += kPartThreads) {
-      if (i < nrows)
-        cp_async_ca<kTs>(g + kTs * i, in + orow[i]);
-      else
-        cp_async16(ge + 16 * i,
-                   reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(out + gext[i - nrows]) &
-                                                 ~uintptr_t(15)));
-    }
-  };
 
-  // One row of the next block, loaded into registers before its barrier:
-  // after the barrier a row only reads its dependencies' values and runs its
-  // multiply-subtract chain.
+  if (tid >= kPartThreads) {
+    // ---- producer warps: records kRing blocks ahead of the consumers, the
+    // gathers of a block kAhead loop steps after its record
+    const int pt = tid - kPartThreads;
+    for (int k = 0; k < nb + kAhead; ++k) {
+      if (k < nb) {
+        if (k >= kRing && !mbar_wait(&empty[k % kRing], ((k / kRing) - 1) & 1, limit)) {
+          atomicCAS(err, 0, (int)MTLGPU_TIMEOUT);
+          abort_flag = 1;
+          break;
+        }
+        if (pt == 0) {  // the record: one bulk copy
+          const unsigned bytes = (unsigned)(offs[k + 1] - offs[k]) * 16u;
+          mbar_arrive_expect_tx(&rec_full[k % kRing], bytes);
+          bulk_copy_g2s(slot(k), recs + (size_t)offs[k] * 16, bytes, &rec_full[k % kRing]);
+        }
+      }
+      const int j = k - kAhead;
+      if (j >= 0) {
+        if (!mbar_wait(&rec_full[j % kRing], (j / kRing) & 1, limit)) {
+          atomicCAS(err, 0, (int)MTLGPU_TIMEOUT);
+          abort_flag = 1;
+          break;
+        }
+        // right-hand sides at element size (the input is not written during
+        // the sweep), external values as 16-byte chunks through L2
+        unsigned char* s = slot(j);
+        const RecHdr& h = *reinterpret_cast<const RecHdr*>(s);
+        const int nrows = h.nrows, ng = h.nrows + h.next;
+        const int* orow = reinterpret_cast<const int*>(s + 48);
+        const int* gext = reinterpret_cast<const int*>(s + h.off_gext);
+        unsigned char* g = s + h.bytes;
+        unsigned char* ge = g + a16(kTs * nrows) - 16 * nrows;
+        for (int i = pt; i < ng; i += kProducers) {
+          if (i < nrows)
+            cp_async_ca<kTs>(g + kTs * i, in + orow[i]);
+          else
+            cp_async16(ge + 16 * i, reinterpret_cast<const void*>(
+                                        reinterpret_cast<uintptr_t>(out + gext[i - nrows]) &
+                                        ~uintptr_t(15)));
+        }
+        mbar_arrive_cp_async(&full[j % kRing]);
+      }
+    }
+    cp_async_wait<0>();
+    return;
+  }
+
+  // ---- consumer warps: one row per thread and block
+  const int lane = tid & 31;
   struct Row {
-    int nrows = 0, slot0 = 0, K = 0, out_idx = 0, over = 0;
+    int nrows = 0, slot0 = 0, out_idx = 0, over = 0;
     T rhs = T(0), dia = T(1);
     int ref[kRegEnt];
     T val[kRegEnt];
     T wext[kRegEnt];  // prefetched external value (sentinel: not ready then)
   };
+  // Block k's row for this thread, into registers before the block's barrier.
   auto load_row = [&](int k, Row& R) {
     const unsigned char* s = slot(k);
     const RecHdr h = *reinterpret_cast<const RecHdr*>(s);
     R.nrows = h.nrows;
     R.slot0 = h.slot0;
-    R.K = h.K;
     if (tid >= h.nrows) return;
     R.out_idx = reinterpret_cast<const int*>(s + 48)[tid];
     R.rhs = reinterpret_cast<const T*>(s + h.bytes)[tid];
@@ -215,25 +304,24 @@ __global__ void __launch_bounds__(kPartThreads, 1)
     }
   };
 
-  // prologue: records of blocks 0 .. kRing-2, then the first kAhead gathers
-  for (int k = 0; k < kRing - 1 && k < nb; ++k) copy_rec(k);
-  cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  for (int k = 0; k < kAhead; ++k) {
-    if (k < nb) gather(k);
-    cp_async_commit();
-  }
   Row R;
-  cp_async_wait<kAhead - 1>();
-  __syncthreads();
-  if (nb > 0) load_row(0, R);
-
+  if (nb > 0) {
+    if (!(mbar_wait(&rec_full[0], 0, limit) && mbar_wait(&full[0], 0, limit))) {
+      atomicCAS(err, 0, (int)MTLGPU_TIMEOUT);
+      abort_flag = 1;
+    }
+    consumer_sync();
+    if (!abort_flag) load_row(0, R);
+  }
   for (int t = 0; t < nb; ++t) {
-    // Block t+1's gathers have landed (and, earlier, its record); the values
-    // of block t-1 are in shared memory; nobody reads block t-1's slot again.
-    cp_async_wait<kAhead - 2>();
-    __syncthreads();
+    // Block t+1 has landed; the values of block t-1 are in shared memory.
+    if (t + 1 < nb && !(mbar_wait(&rec_full[(t + 1) % kRing], ((t + 1) / kRing) & 1, limit) &&
+                        mbar_wait(&full[(t + 1) % kRing], ((t + 1) / kRing) & 1, limit))) {
+      atomicCAS(err, 0, (int)MTLGPU_TIMEOUT);
+      abort_flag = 1;
+    }
+    consumer_sync();
+    if (abort_flag) break;
     if (tid < R.nrows) {
       T w[kRegEnt];
 #pragma unroll
@@ -243,9 +331,10 @@ __global__ void __launch_bounds__(kPartThreads, 1)
       for (int q = 0; q < kRegEnt; ++q) {
         if (R.ref[q] != kNoEntry) {
           if (R.ref[q] < 0 && Box<T>::is(w[q])) {  // not ready when gathered: poll
-            const RecHdr& h = *reinterpret_cast<const RecHdr*>(slot(t));
+            const unsigned char* s = slot(t);
             const int e = (-R.ref[q] - 1) >> 2;
-            w[q] = wait_value(out + reinterpret_cast<const int*>(slot(t) + h.off_gext)[e], limit, err);
+            const int off_gext = reinterpret_cast<const RecHdr*>(s)->off_gext;
+            w[q] = wait_value(out + reinterpret_cast<const int*>(s + off_gext)[e], limit, err);
           }
           rr = sub_rn(rr, mul_rn(R.val[q], w[q]));
         }
@@ -254,7 +343,8 @@ __global__ void __launch_bounds__(kPartThreads, 1)
         const unsigned char* s = slot(t);
         const RecHdr& h = *reinterpret_cast<const RecHdr*>(s);
         const int* oref = reinterpret_cast<const int*>(s + h.off_over + a16(4 * h.nrows));
-        const T* oval = reinterpret_cast<const T*>(s + h.off_over + a16(4 * h.nrows) + a16(4 * h.nover));
+        const T* oval =
+            reinterpret_cast<const T*>(s + h.off_over + a16(4 * h.nrows) + a16(4 * h.nover));
         const int* gext = reinterpret_cast<const int*>(s + h.off_gext);
         const unsigned char* ge = s + h.bytes + a16(kTs * h.nrows);
         const int e0 = R.over >> 8, e1 = e0 + (R.over & 255);
@@ -275,12 +365,10 @@ __global__ void __launch_bounds__(kPartThreads, 1)
       vals[R.slot0 + tid] = rr;
       st_relaxed(out + R.out_idx, rr);
     }
-    if (t + kRing - 1 < nb) copy_rec(t + kRing - 1);
-    if (t + kAhead < nb) gather(t + kAhead);
-    cp_async_commit();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[t % kRing]);  // this warp is done with slot t
     if (t + 1 < nb) load_row(t + 1, R);
   }
-  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -708,17 +796,21 @@ mtlgpu_status part_plan_build(Ctx* ctx, SweepPlan* S, bool with_fp32) {
                                          cudaMemcpyHostToDevice, ctx->stream));
     int occ = 0;
     if (prec == 0) {
+      cudaFuncAttributes fa{};
+      MTLGPU_TRY_CUDA(ctx, cudaFuncGetAttributes(&fa, part_sweep_kernel<double>));
       MTLGPU_TRY_CUDA(ctx, cudaFuncSetAttribute(part_sweep_kernel<double>,
                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                in.smem_optin));
+                                                in.smem_optin - (int)fa.sharedSizeBytes));
       MTLGPU_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                               &occ, part_sweep_kernel<double>, kPartThreads, V.smem_bytes));
+                               &occ, part_sweep_kernel<double>, kCtaThreads, V.smem_bytes));
     } else {
+      cudaFuncAttributes fa{};
+      MTLGPU_TRY_CUDA(ctx, cudaFuncGetAttributes(&fa, part_sweep_kernel<float>));
       MTLGPU_TRY_CUDA(ctx, cudaFuncSetAttribute(part_sweep_kernel<float>,
                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                in.smem_optin));
+                                                in.smem_optin - (int)fa.sharedSizeBytes));
       MTLGPU_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                               &occ, part_sweep_kernel<float>, kPartThreads, V.smem_bytes));
+                               &occ, part_sweep_kernel<float>, kCtaThreads, V.smem_bytes));
     }
     MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // host buffers die after this
     // one resident CTA per part, all at once
@@ -758,7 +850,7 @@ mtlgpu_status part_sweep_launch(Ctx* ctx, const SweepPlan& S, const T* in, T* ou
                                 const int* skip) {
   const auto& V = S.part->prec[sizeof(T) == 8 ? 0 : 1];
   ctx->launches++;
-  part_sweep_kernel<T><<<S.part->P, kPartThreads, V.smem_bytes, ctx->stream>>>(
+  part_sweep_kernel<T><<<S.part->P, kCtaThreads, V.smem_bytes, ctx->stream>>>(
       V.d_part_blk, V.d_blk_off16, V.d_rec, V.vals_bytes, V.offs_bytes, V.slot_bytes, in, out,
       ctx->d_error, ctx->spin_limit, skip);
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
