@@ -270,6 +270,23 @@ mtlgpu_status mtlgpu_solve_host(int method, mtlgpu_csr* A, mtlgpu_pc* P, double*
                                 mtlgpu_iter_result* res);
 void mtlgpu_iter_params_default(mtlgpu_iter_params* p);
 
+/* Batched PCG: `count` independent systems in one solve.  Each system s is
+ * the diagonal block of rows/columns [h_offsets[s], h_offsets[s+1]) of the
+ * block-diagonal matrix A (h_offsets: host array of count+1, from 0 to the
+ * row count; a row referencing a column outside its block is rejected with
+ * MTLGPU_INVALID_ARG) and follows itl::cg(A_s, x_s, b_s, P_s, iter_s)
+ * (cg.hpp:75-112) with iter_s = basic_iteration(b_s, max_iter, rtol, atol)
+ * (basic_iteration.hpp:31-39): its own scalars, iteration count and stopping
+ * test.  P may be NULL (identity) or a diagonal / ic_0 / ilu_0 preconditioner
+ * of A (factorising a block-diagonal matrix factorises each block).  Only
+ * MTLGPU_CG and FP64 mode.  h_results (host, count entries) receives each
+ * system's iteration state; the call returns MTLGPU_MAX_ITER when any system
+ * stopped on max_iter. */
+mtlgpu_status mtlgpu_solve_batched(int method, mtlgpu_csr* A, mtlgpu_pc* P, int count,
+                                   const int32_t* h_offsets, double* d_x, const double* d_b,
+                                   const mtlgpu_iter_params* params,
+                                   mtlgpu_iter_result* h_results);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

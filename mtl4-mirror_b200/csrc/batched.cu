@@ -1,0 +1,299 @@
+// Batched PCG: many independent SPD systems in one solve.
+//
+// Each system s follows itl::cg(A_s, x_s, b_s, P_s, iter_s) (itl/krylov/
+// cg.hpp:75-112) with iter_s = basic_iteration(b_s, max_iter, rtol, atol)
+// (itl/iteration/basic_iteration.hpp:31-39): the systems are the diagonal
+// blocks of one block-diagonal CSR matrix, so the preconditioner (Jacobi,
+// IC(0), ILU(0): no fill crosses a block) and the SpMV run once over all of
+// them, while every system keeps its own scalars (rho, alpha, beta, the
+// residual, its iteration count and its stopping decision) in device memory.
+//
+// Kernels: one CTA per system for everything that reduces over a system --
+// rho = r.z with p = z + beta p, and p.q with x += alpha p, r -= alpha q and
+// r.r -- so a system's reductions need no cross-CTA step and are
+// deterministic.  A system that has stopped keeps its x; its CTAs return at
+// once.  The host checks a stopped-systems counter every few iterations.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace mtlgpu {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kBlock = 256;
+
+struct BatchSys {
+  double rho, rr, norm_b, resid;
+  int it, done, error, pad;
+};
+
+__device__ __forceinline__ double block_sum(double v) {
+  Sum<1> a = Sum<1>::zero();
+  a.add(0, v);
+  return block_reduce(a).value(0);
+}
+
+__device__ __forceinline__ bool converged(const BatchSys& S, double resid, double rtol,
+                                          double atol) {
+  return S.norm_b == 0 ? resid <= atol : (resid <= rtol * S.norm_b || resid <= atol);
+}
+
+// Rows of system s must only reference columns of system s.
+__global__ void __launch_bounds__(kBlock)
+    batch_check_kernel(const int32_t* __restrict__ off, const int32_t* __restrict__ rp,
+                       const int32_t* __restrict__ ci, int* err) {
+  const int s = blockIdx.x, lo = off[s], hi = off[s + 1];
+  for (int r = lo + threadIdx.x; r < hi; r += blockDim.x)
+    for (int j = rp[r]; j < rp[r + 1]; ++j)
+      if (ci[j] < lo || ci[j] >= hi) atomicCAS(err, 0, (int)MTLGPU_INVALID_ARG);
+}
+
+// r = b - A x (Ax given), rr, ||b||; the loop-top termination test.
+__global__ void __launch_bounds__(kBlock)
+    batch_init_kernel(const int32_t* __restrict__ off, const double* __restrict__ b,
+                      const double* __restrict__ ax, double* __restrict__ r, BatchSys* sys,
+                      double rtol, double atol, int max_iter, unsigned* n_done) {
+  const int s = blockIdx.x, lo = off[s], hi = off[s + 1];
+  double rr = 0, bb = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double v = b[i] - ax[i];
+    r[i] = v;
+    rr += v * v;
+    bb += b[i] * b[i];
+  }
+  rr = block_sum(rr);
+  __syncthreads();
+  bb = block_sum(bb);
+  if (threadIdx.x == 0) {
+    BatchSys S{};
+    S.rr = rr;
+    S.norm_b = sqrt(bb);
+    S.resid = sqrt(fabs(rr));
+    if (converged(S, S.resid, rtol, atol)) {
+      S.done = 1;
+    } else if (max_iter <= 0) {
+      S.done = 1;
+      S.error = 1;
+    }
+    if (S.done) atomicAdd(n_done, 1u);
+    sys[s] = S;
+  }
+}
+
+// ++iter; rho = r.z; p = z (first iteration) or z + (rho / rho_1) p
+__global__ void __launch_bounds__(kBlock)
+    batch_rho_p_kernel(const int32_t* __restrict__ off, const double* __restrict__ r,
+                       const double* __restrict__ z, double* __restrict__ p, BatchSys* sys) {
+  const int s = blockIdx.x;
+  if (sys[s].done) return;
+  const int lo = off[s], hi = off[s + 1];
+  double rho = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) rho += r[i] * z[i];
+  rho = block_sum(rho);
+  __shared__ double beta_s;
+  __shared__ int first_s;
+  if (threadIdx.x == 0) {
+    BatchSys& S = sys[s];
+    S.it += 1;
+    first_s = S.it <= 1;
+    beta_s = first_s ? 0.0 : rho / S.rho;
+    S.rho = rho;
+  }
+  __syncthreads();
+  const double beta = beta_s;
+  if (first_s) {
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) p[i] = z[i];
+  } else {
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) p[i] = z[i] + beta * p[i];
+  }
+}
+
+// alpha = rho / p.q; x += alpha p; r -= alpha q; rr = r.r; termination test
+__global__ void __launch_bounds__(kBlock)
+    batch_update_kernel(const int32_t* __restrict__ off, const double* __restrict__ p,
+                        const double* __restrict__ q, double* __restrict__ x,
+                        double* __restrict__ r, BatchSys* sys, double rtol, double atol,
+                        int max_iter, unsigned* n_done) {
+  const int s = blockIdx.x;
+  if (sys[s].done) return;
+  const int lo = off[s], hi = off[s + 1];
+  double pq = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) pq += p[i] * q[i];
+  pq = block_sum(pq);
+  __shared__ double alpha_s;
+  if (threadIdx.x == 0) alpha_s = sys[s].rho / pq;
+  __syncthreads();
+  const double alpha = alpha_s;
+  double rr = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    x[i] += alpha * p[i];
+    const double v = r[i] - alpha * q[i];
+    r[i] = v;
+    rr += v * v;
+  }
+  rr = block_sum(rr);
+  if (threadIdx.x == 0) {
+    BatchSys& S = sys[s];
+    S.rr = rr;
+    S.resid = sqrt(fabs(rr));
+    if (converged(S, S.resid, rtol, atol)) {
+      S.done = 1;
+    } else if (S.it >= max_iter) {
+      S.done = 1;
+      S.error = 1;
+    }
+    if (S.done) atomicAdd(n_done, 1u);
+  }
+}
+
+// ||b - A x|| per system (Ax given)
+__global__ void __launch_bounds__(kBlock)
+    batch_true_resid_kernel(const int32_t* __restrict__ off, const double* __restrict__ b,
+                            const double* __restrict__ ax, double* out) {
+  const int s = blockIdx.x, lo = off[s], hi = off[s + 1];
+  double rr = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double v = b[i] - ax[i];
+    rr += v * v;
+  }
+  rr = block_sum(rr);
+  if (threadIdx.x == 0) out[s] = sqrt(rr);
+}
+
+}  // namespace
+
+mtlgpu_status solve_batched_impl(int method, Csr* A, Pc* P, int count, const int32_t* h_off,
+                                 double* d_x, const double* d_b, const mtlgpu_iter_params* prm,
+                                 mtlgpu_iter_result* res) {
+  Ctx* ctx = A->ctx;
+  if (method != MTLGPU_CG) return MTLGPU_NOT_SUPPORTED;
+  if (count <= 0 || !h_off || !d_x || !d_b || !prm || !res) return MTLGPU_INVALID_ARG;
+  if (A->n_rows != A->n_cols) return MTLGPU_NOT_SQUARE;
+  if (P && P->A != A) return MTLGPU_INVALID_ARG;
+  if (h_off[0] != 0 || h_off[count] != A->n_rows) return MTLGPU_INCOMPATIBLE_SIZE;
+  for (int s = 0; s < count; ++s)
+    if (h_off[s + 1] < h_off[s]) return MTLGPU_INVALID_ARG;
+  const int n = A->n_rows;
+  const double rtol = prm->rtol, atol = prm->atol;
+  const int max_iter = prm->max_iter;
+
+  int32_t* d_off = nullptr;
+  double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *d_tr = nullptr;
+  BatchSys* sys = nullptr;
+  unsigned* n_done = nullptr;
+  unsigned* h_done = nullptr;
+  mtlgpu_status st = MTLGPU_OK;
+  auto cleanup = [&]() {
+    dfree(ctx, d_off);
+    dfree(ctx, r);
+    dfree(ctx, z);
+    dfree(ctx, p);
+    dfree(ctx, q);
+    dfree(ctx, d_tr);
+    dfree(ctx, sys);
+    dfree(ctx, n_done);
+    if (h_done) cudaFreeHost(h_done);
+  };
+#define MTLGPU_BTRY(call)            \
+  do {                               \
+    st = (call);                     \
+    if (st != MTLGPU_OK) {           \
+      cleanup();                     \
+      return st;                     \
+    }                                \
+  } while (0)
+#define MTLGPU_BTRY_CUDA(call) MTLGPU_BTRY(((call) == cudaSuccess) ? MTLGPU_OK : set_cuda_error(ctx, cudaGetLastError(), #call))
+
+  MTLGPU_BTRY(dalloc(ctx, &d_off, count + 1));
+  MTLGPU_BTRY(dalloc(ctx, &r, n));
+  MTLGPU_BTRY(dalloc(ctx, &z, n));
+  MTLGPU_BTRY(dalloc(ctx, &p, n));
+  MTLGPU_BTRY(dalloc(ctx, &q, n));
+  MTLGPU_BTRY(dalloc(ctx, &d_tr, count));
+  MTLGPU_BTRY(dalloc(ctx, &sys, count));
+  MTLGPU_BTRY(dalloc(ctx, &n_done, 1));
+  MTLGPU_BTRY_CUDA(cudaMallocHost(&h_done, sizeof(unsigned)));
+  MTLGPU_BTRY_CUDA(cudaMemcpyAsync(d_off, h_off, sizeof(int32_t) * (count + 1),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  MTLGPU_BTRY_CUDA(cudaMemsetAsync(n_done, 0, sizeof(unsigned), ctx->stream));
+  MTLGPU_BTRY_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * n, ctx->stream));
+  batch_check_kernel<<<count, kBlock, 0, ctx->stream>>>(d_off, A->d_rp, A->d_ci, ctx->d_error);
+  ctx->launches++;
+  MTLGPU_BTRY(take_device_error(ctx));
+
+  SpmvArgs plain;
+  MTLGPU_BTRY(spmv_launch<double>(A, d_x, q, plain));
+  batch_init_kernel<<<count, kBlock, 0, ctx->stream>>>(d_off, d_b, q, r, sys, rtol, atol, max_iter,
+                                                       n_done);
+  ctx->launches++;
+  // Each loop step is one CG iteration of every running system.
+  for (int k = 0; k < max_iter; ++k) {
+    if ((k & 7) == 0) {
+      MTLGPU_BTRY_CUDA(cudaMemcpyAsync(h_done, n_done, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+      MTLGPU_BTRY_CUDA(cudaStreamSynchronize(ctx->stream));
+      if ((int)*h_done >= count) break;
+      if (prm->h_interrupt && *prm->h_interrupt) {
+        st = MTLGPU_INTERRUPTED;
+        break;
+      }
+    }
+    if (P && P->kind != MTLGPU_PC_IDENTITY) {
+      MTLGPU_BTRY(pc_apply_t<double>(P, r, z, false, nullptr, false, false));
+    } else {
+      MTLGPU_BTRY_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+    }
+    batch_rho_p_kernel<<<count, kBlock, 0, ctx->stream>>>(d_off, r, z, p, sys);
+    MTLGPU_BTRY(spmv_launch<double>(A, p, q, plain));
+    batch_update_kernel<<<count, kBlock, 0, ctx->stream>>>(d_off, p, q, d_x, r, sys, rtol, atol,
+                                                           max_iter, n_done);
+    ctx->launches += 2;
+    MTLGPU_BTRY_CUDA(cudaGetLastError());
+  }
+  // true residuals and the per-system results
+  MTLGPU_BTRY(spmv_launch<double>(A, d_x, q, plain));
+  batch_true_resid_kernel<<<count, kBlock, 0, ctx->stream>>>(d_off, d_b, q, d_tr);
+  ctx->launches++;
+  std::vector<BatchSys> hs(count);
+  std::vector<double> htr(count);
+  MTLGPU_BTRY_CUDA(cudaMemcpyAsync(hs.data(), sys, sizeof(BatchSys) * count,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  MTLGPU_BTRY_CUDA(cudaMemcpyAsync(htr.data(), d_tr, sizeof(double) * count,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  MTLGPU_BTRY_CUDA(cudaStreamSynchronize(ctx->stream));
+  MTLGPU_BTRY(take_device_error(ctx));
+  bool any_max = false;
+  for (int s = 0; s < count; ++s) {
+    mtlgpu_iter_result& R = res[s];
+    std::memset(&R, 0, sizeof(R));
+    R.iterations = hs[s].it;
+    R.error = hs[s].done ? hs[s].error : 1;
+    R.status = R.error ? MTLGPU_MAX_ITER : (st == MTLGPU_INTERRUPTED ? MTLGPU_INTERRUPTED : MTLGPU_OK);
+    R.resid = hs[s].resid;
+    R.norm_r0 = hs[s].norm_b;
+    R.true_resid = htr[s];
+    any_max |= R.error != 0;
+  }
+  cleanup();
+#undef MTLGPU_BTRY
+#undef MTLGPU_BTRY_CUDA
+  if (st == MTLGPU_INTERRUPTED) return st;
+  return any_max ? MTLGPU_MAX_ITER : MTLGPU_OK;
+}
+
+}  // namespace mtlgpu
+
+extern "C" mtlgpu_status mtlgpu_solve_batched(int method, mtlgpu_csr* A, mtlgpu_pc* P, int count,
+                                              const int32_t* h_offsets, double* d_x,
+                                              const double* d_b, const mtlgpu_iter_params* params,
+                                              mtlgpu_iter_result* h_results) {
+  if (!A) return MTLGPU_INVALID_ARG;
+  return mtlgpu::solve_batched_impl(method, A, P, count, h_offsets, d_x, d_b, params, h_results);
+}

@@ -310,7 +310,7 @@ class Pc:
 
 
 def make_params(max_iter=1000, rtol=1e-10, atol=0.0, norm_r0=-1.0, mode=SOLVE_FP64,
-                inner_rtol=1e-4, inner_max_iter=0, max_outer=0, history=None, interrupt=None):
+                inner_rtol=0.0, inner_max_iter=0, max_outer=0, history=None, interrupt=None):
     p = IterParams()
     _lib().mtlgpu_iter_params_default(C.byref(p))
     p.max_iter, p.rtol, p.atol, p.norm_r0, p.mode = max_iter, rtol, atol, norm_r0, mode
@@ -331,6 +331,18 @@ def solve(method, A, P, x, b, **kw):
     st = _lib().mtlgpu_solve(METHODS.get(method, method), A.h, P.h if P else None, x.ptr, b.ptr,
                              C.byref(prm), C.byref(res))
     return st, res, hist[:min(res.history_len, len(hist))].copy()
+
+
+def solve_batched(A, P, offsets, x, b, **kw):
+    """Batched itl::cg over the diagonal blocks [offsets[s], offsets[s+1]) of the
+    block-diagonal device matrix A; returns (status, list of IterResult)."""
+    off = np.ascontiguousarray(offsets, np.int32)
+    count = len(off) - 1
+    prm = make_params(**kw)
+    res = (IterResult * count)()
+    st = _lib().mtlgpu_solve_batched(METHODS["cg"], A.h, P.h if P else None, count, _p(off),
+                                     x.ptr, b.ptr, C.byref(prm), res)
+    return st, list(res)
 
 
 def solve_host(method, A, P, x, b, **kw):
@@ -391,6 +403,36 @@ def random_graph(n, avg_deg, shift_frac=1e-2, seed=3):
     rp, ci, v = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
     L.mtlgpu_gen_random_graph(n, avg_deg, shift_frac, seed, _p(rp), _p(ci), _p(v))
     return (n, rp, ci, v)
+
+
+def graph_batch(count, n_min=1000, n_max=65536, deg_min=8.0, deg_max=32.0, shift_frac=1e-2,
+                seed=3):
+    """`count` random-graph Laplacians of log-uniform sizes (the batched-PCG
+    workload): returns (systems, blockdiag) with systems a list of
+    (n, rp, ci, v) and blockdiag = (n_total, rp, ci, v, offsets)."""
+    L = _lib()
+    sizes = np.zeros(2 * count, np.int64)
+    total = L.mtlgpu_gen_graph_batch(count, n_min, n_max, deg_min, deg_max, shift_frac, seed,
+                                     _p(sizes), None, None, None)
+    ns, nz = sizes[0::2], sizes[1::2]
+    rp = np.zeros(int(ns.sum() + count), np.int32)
+    ci, v = np.zeros(total, np.int32), np.zeros(total)
+    L.mtlgpu_gen_graph_batch(count, n_min, n_max, deg_min, deg_max, shift_frac, seed, _p(sizes),
+                             _p(rp), _p(ci), _p(v))
+    systems, ro, eo = [], 0, 0
+    for s in range(count):
+        n, m = int(ns[s]), int(nz[s])
+        systems.append((n, rp[ro:ro + n + 1].copy(), ci[eo:eo + m].copy(), v[eo:eo + m].copy()))
+        ro, eo = ro + n + 1, eo + m
+    offsets = np.concatenate([[0], np.cumsum(ns)]).astype(np.int32)
+    brp = np.zeros(int(offsets[-1]) + 1, np.int32)
+    bci = np.zeros(total, np.int32)
+    e = 0
+    for s, (n, srp, sci, sv) in enumerate(systems):
+        brp[offsets[s] + 1:offsets[s + 1] + 1] = srp[1:] + e
+        bci[e:e + len(sci)] = sci + offsets[s]
+        e += len(sci)
+    return systems, (int(offsets[-1]), brp, bci, v, offsets)
 
 
 def fv2d(N, sigma=1.0, corr=8.0, seed=4):
