@@ -175,6 +175,17 @@ mtlgpu_status mtlgpu_csr_info(const mtlgpu_csr* A, int* n_rows, int* n_cols, int
 /* Device views of the arrays (read-only for the caller). */
 mtlgpu_status mtlgpu_csr_device_arrays(const mtlgpu_csr* A, const int32_t** d_row_ptr,
                                        const int32_t** d_col_idx, const double** d_vals);
+/* A^T as a new handle (rows sorted by column), for adjoint solves of an
+ * unsymmetric A (trans(A), transposed_sparse_matrix_vector_product_test.cpp:32). */
+mtlgpu_status mtlgpu_csr_create_transpose(mtlgpu_csr* A, mtlgpu_csr** out);
+/* Gradient of a loss with respect to A's stored values in the solve
+ * x = A^{-1} b, given the adjoint d_lambda (A^T lambda = dL/dx):
+ * d_grad[k] = -lambda[i] * x[j] for the k-th stored entry (i, j).  The
+ * gradient with respect to b is lambda itself.  No counterpart in the
+ * reference (differentiation is not part of MTL4). */
+mtlgpu_status mtlgpu_csr_values_grad(mtlgpu_csr* A, const double* d_lambda, const double* d_x,
+                                     double* d_grad);
+
 /* Choose SpMV row-bin thresholds by timing the candidates on this matrix
  * (kept on the handle; reported in *h_choice when non-NULL). */
 mtlgpu_status mtlgpu_csr_autotune(mtlgpu_csr* A, int* h_choice);

@@ -705,6 +705,80 @@ struct refinement {
       : inner_rtol(rtol), inner_max_iter(inner_max), max_outer(outer) {}
 };
 
+/// Differentiable solve x = A^{-1} b with autograd-Function semantics and no
+/// PyTorch dependency: forward(b) solves and keeps x; backward(dL/dx) solves
+/// the adjoint A^T lambda = dL/dx with the same preconditioned Krylov path
+/// and returns dL/db = lambda and dL/dvals(A)[k] = -lambda_i x_j for every
+/// stored entry k = (i, j) of A.  symmetric = true: CG on A for both solves
+/// (A^T = A); false: BiCGSTAB on A and on A^T (a transposed handle and its
+/// own preconditioner).
+class linear_solve {
+ public:
+  explicit linear_solve(const compressed2D<double>& A, int pc_kind = MTLGPU_PC_IC0,
+                        bool symmetric = true, double rtol = 1e-12, int max_iter = 10000)
+      : A_(&A), sym_(symmetric), rtol_(rtol), max_iter_(max_iter), x_(A.num_rows(), A.ctx()) {
+    mtlgpu_ctx* c = A.ctx().get();
+    P_ = make_pc(A.handle(), pc_kind, c);
+    if (!symmetric) {
+      mtlgpu_csr* t = nullptr;
+      throw_on(mtlgpu_csr_create_transpose(A.handle(), &t), c);
+      AT_.reset(t, [](mtlgpu_csr* q) { mtlgpu_csr_destroy(q); });
+      PT_ = make_pc(t, pc_kind, c);
+    }
+  }
+  /// x = A^{-1} b (kept for backward)
+  const dense_vector<double>& forward(const dense_vector<double>& b) {
+    x_ = 0.0;
+    fwd_it_ = solve(A_->handle(), P_.get(), x_, b);
+    return x_;
+  }
+  /// dL/db and dL/dvals(A) from dL/dx at the last forward solution
+  void backward(const dense_vector<double>& dl_dx, dense_vector<double>& grad_b,
+                dense_vector<double>& grad_vals) {
+    if (grad_vals.size() != A_->nnz() || grad_b.size() != A_->num_rows())
+      throw mtl::incompatible_size();
+    grad_b = 0.0;
+    bwd_it_ = sym_ ? solve(A_->handle(), P_.get(), grad_b, dl_dx)
+                   : solve(AT_.get(), PT_.get(), grad_b, dl_dx);
+    throw_on(mtlgpu_csr_values_grad(A_->handle(), grad_b.data(), x_.data(), grad_vals.data()),
+             A_->ctx().get());
+  }
+  const dense_vector<double>& x() const { return x_; }
+  int forward_iterations() const { return fwd_it_; }
+  int backward_iterations() const { return bwd_it_; }
+
+ private:
+  static std::shared_ptr<mtlgpu_pc> make_pc(mtlgpu_csr* M, int kind, mtlgpu_ctx* c) {
+    if (kind == MTLGPU_PC_IDENTITY) return nullptr;
+    mtlgpu_pc* P = nullptr;
+    const int st = mtlgpu_pc_create(M, kind, MTLGPU_FP64, &P);
+    std::shared_ptr<mtlgpu_pc> h(P, [](mtlgpu_pc* q) {
+      if (q) mtlgpu_pc_destroy(q);
+    });
+    throw_on(st, c);
+    return h;
+  }
+  int solve(mtlgpu_csr* M, mtlgpu_pc* P, dense_vector<double>& x, const dense_vector<double>& b) {
+    mtlgpu_iter_params p;
+    mtlgpu_iter_params_default(&p);
+    p.max_iter = max_iter_;
+    p.rtol = rtol_;
+    mtlgpu_iter_result r;
+    const int st = mtlgpu_solve(sym_ ? MTLGPU_CG : MTLGPU_BICGSTAB, M, P, x.data(), b.data(), &p, &r);
+    if (st == MTLGPU_MAX_ITER) throw mtl::runtime_error("linear_solve: iteration limit reached");
+    throw_on(st, A_->ctx().get());
+    return r.iterations;
+  }
+  const compressed2D<double>* A_;
+  bool sym_;
+  double rtol_;
+  int max_iter_;
+  dense_vector<double> x_;
+  std::shared_ptr<mtlgpu_pc> P_, PT_;
+  std::shared_ptr<mtlgpu_csr> AT_;
+  int fwd_it_ = 0, bwd_it_ = 0;
+};
+
 namespace detail {
 
 template <typename Pc>

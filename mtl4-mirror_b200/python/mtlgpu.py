@@ -228,6 +228,18 @@ class Csr:
         v = np.ascontiguousarray(v, np.float64)
         check(_lib().mtlgpu_csr_set_values(self.h, _p(v), None), "csr_set_values")
 
+    def transpose(self):
+        """A^T as a new handle (mtlgpu_csr_create_transpose)."""
+        T = Csr.__new__(Csr)
+        T.ctx, T.n, T.n_cols, T.nnz = self.ctx, self.n_cols, self.n, self.nnz
+        T.h = _vp()
+        check(_lib().mtlgpu_csr_create_transpose(self.h, C.byref(T.h)), "csr_create_transpose")
+        return T
+
+    def values_grad(self, lam, x, grad):
+        """grad[k] = -lam[i] x[j] for the k-th stored entry (i, j)."""
+        check(_lib().mtlgpu_csr_values_grad(self.h, lam.ptr, x.ptr, grad.ptr), "csr_values_grad")
+
     def spmv(self, x, y, alpha=1.0, beta=0.0):
         check(_lib().mtlgpu_spmv(self.h, x.ptr, y.ptr, float(alpha), float(beta)), "spmv")
 

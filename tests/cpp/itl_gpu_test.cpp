@@ -13,9 +13,11 @@
 //   itl_gpu_test bicgstab    BiCGSTAB + ILU(0) on a 27-point operator
 //   itl_gpu_test mixed       PCG-IC(0) with FP32 inner solves + FP64 refinement
 //   itl_gpu_test errors      exceptions for bad input
+//   itl_gpu_test adjoint     linear_solve forward/backward vs finite differences
 #include <mtlgpu/mtl.hpp>
 #include <mtlgpu_fixtures.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <sstream>
@@ -191,6 +193,78 @@ void case_mixed() {
       err, iter.iterations(), iter.resid(), true_rel_resid(h, x.to_host(), bh));
 }
 
+// Differentiable solve on the 2-D finite-volume operator (N x N, log-normal
+// kappa): L = 1/2 ||x - x_target||^2, x = A^{-1} b with b a Gaussian source and
+// x_target = x + 0.01 N(0,1).  Gradients from linear_solve::backward against
+// central finite differences (h = 1e-6) along random directions in b and in
+// A's values (perturbations kept symmetric, so A stays SPD for CG).
+void case_adjoint() {
+  const int N = 32, n = N * N;
+  HostCsr h;
+  h.n = n;
+  const long long nnz = mtlgpu_gen_fv2d(N, 1.0, 8.0, 4, nullptr, nullptr, nullptr);
+  h.rp.resize(n + 1);
+  h.ci.resize(nnz);
+  h.v.resize(nnz);
+  mtlgpu_gen_fv2d(N, 1.0, 8.0, 4, h.rp.data(), h.ci.data(), h.v.data());
+  std::vector<double> bh(n), noise(n);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      const double x = (i + 0.5) / N - 0.5, y = (j + 0.5) / N - 0.5;
+      bh[i * N + j] = std::exp(-(x * x + y * y) / (2 * 0.1 * 0.1));
+    }
+  mtlgpu_gen_normal(n, 44, noise.data());
+  auto loss_of = [&](const std::vector<double>& vals, const std::vector<double>& b,
+                     const std::vector<double>& xt) {
+    Matrix A(n, n, (int)nnz, h.rp.data(), h.ci.data(), vals.data());
+    mtl::gpu::linear_solve S(A, MTLGPU_PC_IC0, true, 1e-14, 20000);
+    std::vector<double> x = S.forward(Vector(b)).to_host();
+    double L = 0;
+    for (int i = 0; i < n; ++i) L += 0.5 * (x[i] - xt[i]) * (x[i] - xt[i]);
+    return std::make_pair(L, x);
+  };
+  Matrix A = h.device();
+  mtl::gpu::linear_solve S(A, MTLGPU_PC_IC0, true, 1e-14, 20000);
+  std::vector<double> x = S.forward(Vector(bh)).to_host();
+  std::vector<double> xt(n), dl(n);
+  for (int i = 0; i < n; ++i) xt[i] = x[i] + 0.01 * noise[i];
+  for (int i = 0; i < n; ++i) dl[i] = x[i] - xt[i];
+  Vector gb(n), gv((int)nnz);
+  S.backward(Vector(dl), gb, gv);
+  const std::vector<double> gbh = gb.to_host(), gvh = gv.to_host();
+  // transpose position of every entry (the pattern is symmetric)
+  std::vector<int> tpos(nnz);
+  for (int r = 0; r < n; ++r)
+    for (int k = h.rp[r]; k < h.rp[r + 1]; ++k) {
+      const int c = h.ci[k];
+      for (int m = h.rp[c]; m < h.rp[c + 1]; ++m)
+        if (h.ci[m] == r) tpos[k] = m;
+    }
+  const double eps = 1e-6;
+  double worst_b = 0, worst_v = 0;
+  std::vector<double> dir(n), dv(nnz), tmp(nnz);
+  for (int d = 0; d < 8; ++d) {
+    mtlgpu_gen_normal(n, 100 + d, dir.data());
+    std::vector<double> bp(bh), bm(bh);
+    double pred = 0;
+    for (int i = 0; i < n; ++i) bp[i] += eps * dir[i], bm[i] -= eps * dir[i], pred += gbh[i] * dir[i];
+    const double fd = (loss_of(h.v, bp, xt).first - loss_of(h.v, bm, xt).first) / (2 * eps);
+    worst_b = std::max(worst_b, std::abs(fd - pred) / std::max(std::abs(pred), 1e-30));
+    mtlgpu_gen_normal(nnz, 200 + d, tmp.data());
+    for (long long k = 0; k < nnz; ++k) dv[k] = 0.5 * (tmp[k] + tmp[tpos[k]]);
+    std::vector<double> vp(h.v), vm(h.v);
+    double predv = 0;
+    for (long long k = 0; k < nnz; ++k)
+      vp[k] += eps * dv[k], vm[k] -= eps * dv[k], predv += gvh[k] * dv[k];
+    const double fdv = (loss_of(vp, bh, xt).first - loss_of(vm, bh, xt).first) / (2 * eps);
+    worst_v = std::max(worst_v, std::abs(fdv - predv) / std::max(std::abs(predv), 1e-30));
+  }
+  std::printf(
+      "{\"case\": \"adjoint\", \"forward_iterations\": %d, \"backward_iterations\": %d, "
+      "\"fd_rel_err_b\": %.3e, \"fd_rel_err_vals\": %.3e}\n",
+      S.forward_iterations(), S.backward_iterations(), worst_b, worst_v);
+}
+
 void case_errors() {
   int caught = 0;
   // row 1 has no diagonal entry
@@ -239,6 +313,7 @@ int main(int argc, char** argv) {
     else if (c == "bicgstab") case_bicgstab();
     else if (c == "mixed") case_mixed();
     else if (c == "errors") case_errors();
+    else if (c == "adjoint") case_adjoint();
     else {
       std::fprintf(stderr, "unknown case %s\n", c.c_str());
       return 2;

@@ -101,6 +101,14 @@ def test_exceptions(built):
     assert _run("itl_gpu_test", "errors")["caught"] == 3
 
 
+@pytest.mark.gpu
+def test_linear_solve_gradients_vs_finite_differences(built):
+    r = _run("itl_gpu_test", "adjoint")
+    assert r["forward_iterations"] > 0 and r["backward_iterations"] > 0
+    # central differences with h = 1e-6: truncation and rounding leave ~1e-6 relative
+    assert r["fd_rel_err_b"] <= 5e-5 and r["fd_rel_err_vals"] <= 5e-5, r
+
+
 def _dropin():
     exe = os.path.join(BUILD, "mtl4_dropin")
     if not os.path.exists(exe):
