@@ -163,6 +163,88 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def _local_ms(fn, reps, stream):
+    """Mean ms of fn over reps with CUDA events on `stream` (one GPU)."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = [fn() for _ in range(reps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps, out
+
+
+def batched_workload(M, ctx, stream):
+    """512 independent random-graph Laplacians (n log-uniform in [1e3, 65536],
+    average degree U[8, 32], shift 1e-2 mean degree, seed 3), b ~ N(0,1):
+    one batched PCG to 1e-8 in FP64, Jacobi and IC(0)."""
+    systems, (n, rp, ci, v, off) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2, seed=3)
+    b = M.normal(n, 3)
+    dA = M.Csr(ctx, rp, ci, v)
+    db, dx, dz = ctx.to_device(b), ctx.array(n), ctx.to_device(np.zeros(n))
+    out = {"systems": 512, "n": int(n), "nnz": int(len(ci)), "rtol": 1e-8, "dtype": "f64"}
+    for pc in ("diagonal", "ic0"):
+        P = M.Pc(dA, pc)
+
+        def run():
+            ctx.xpay(dz, 0.0, dx)
+            st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=5000)
+            assert st == M.OK, st
+            return res
+        run()
+        ms, res = _local_ms(run, 2, stream)
+        its = np.array([r.iterations for r in res[-1]])
+        rel = max(r.true_resid / r.norm_r0 for r in res[-1])
+        out[pc] = {"ms": ms, "iterations_max": int(its.max()),
+                   "iterations_mean": float(its.mean()), "max_true_rel_residual": rel}
+        P.close()
+    dA.close()
+    return out
+
+
+def adjoint_workload(M, ctx, stream):
+    """Differentiable solve on the 512 x 512 finite-volume operator (log-normal
+    kappa, sigma 1, 8-cell correlation, seed 4): forward PCG-IC(0) solve,
+    adjoint PCG-IC(0) solve with dL/dx = x - x_target, and the gradient on A's
+    pattern, FP64 to 1e-10."""
+    N = 512
+    A = M.fv2d(N, 1.0, 8.0, 4)
+    n, rp, ci, v = A
+    c = (np.arange(N) + 0.5) / N - 0.5
+    X, Y = np.meshgrid(c, c, indexing="ij")
+    b = np.exp(-(X ** 2 + Y ** 2) / (2 * 0.1 ** 2)).ravel()
+    dA = M.Csr(ctx, rp, ci, v)
+    P = M.Pc(dA, "ic0")
+    db, dx, dz = ctx.to_device(b), ctx.array(n), ctx.to_device(np.zeros(n))
+
+    def forward():
+        ctx.xpay(dz, 0.0, dx)
+        st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=20000)
+        assert st == M.OK, st
+        return res
+    forward()
+    x = dx.download()
+    dg = ctx.to_device(0.01 * M.normal(n, 44) * -1.0)   # x - x_target = -0.01 N(0,1)
+    dlam, grad = ctx.array(n), ctx.array(len(ci))
+
+    def backward():
+        ctx.xpay(dz, 0.0, dlam)
+        st, res, _ = M.solve("cg", dA, P, dlam, dg, rtol=1e-10, max_iter=20000)
+        assert st == M.OK, st
+        dA.values_grad(dlam, dx, grad)
+        return res
+    backward()
+    ms_f, rf = _local_ms(forward, 2, stream)
+    ms_b, rb = _local_ms(backward, 2, stream)
+    out = {"n": int(n), "nnz": int(len(ci)), "forward_ms": ms_f, "backward_ms": ms_b,
+           "forward_iterations": rf[-1].iterations, "backward_iterations": rb[-1].iterations,
+           "dtype": "f64", "rtol": 1e-10}
+    P.close()
+    dA.close()
+    return out
+
+
 def profile_case(case, grid, launches):
     """Runs one kernel of the path a few times on an N^3 Laplacian (for
     profiler captures): 'spmv' (FP64 y = A x), 'sweep64' / 'sweep32' (IC(0)
@@ -194,6 +276,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mtlgpu", choices=["mtlgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and differentiable-solve measurements")
     ap.add_argument("--profile-case", choices=["spmv", "sweep64", "sweep32"])
     ap.add_argument("--grid", type=int, default=64)
     ap.add_argument("--launches", type=int, default=3)
@@ -378,6 +462,9 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if world == 1 and not args.no_extras:
+        line["batched"] = batched_workload(M, ctx, stream)
+        line["differentiable_solve"] = adjoint_workload(M, ctx, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref, kind, cores = reference_solver()
         t, iters, tf = time_reference_solve(ref, kind, A, b)
