@@ -163,6 +163,49 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+class Replicas:
+    """Plumbing of the N-GPU run: one process per GPU, each solving its own
+    replica of the workload (the single-system solve does not shard: see the
+    design notes), a barrier around every timed region, and the slowest rank's
+    time as the job's time.  `dist` is torch.distributed (or None for one
+    process); `device` holds the all-reduce buffer (cuda:<local> with NCCL,
+    cpu with gloo)."""
+
+    def __init__(self, dist, device):
+        self.dist, self.device = dist, device
+
+    @property
+    def rank(self):
+        return self.dist.get_rank() if self.dist is not None else 0
+
+    @property
+    def world(self):
+        return self.dist.get_world_size() if self.dist is not None else 1
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_over_ranks(self, v):
+        if self.dist is None:
+            return v
+        import torch
+        t = torch.tensor([float(v)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def aggregate(self, per_rank_units, ms):
+        """Whole-job throughput: all ranks' units over the slowest rank's time."""
+        return per_rank_units * self.world / (self.max_over_ranks(ms) / 1e3)
+
+    def emit(self, line):
+        """Only rank 0 prints the JSON line."""
+        if self.rank == 0:
+            print(json.dumps(line), flush=True)
+            return True
+        return False
+
+
 def _local_ms(fn, reps, stream):
     """Mean ms of fn over reps with CUDA events on `stream` (one GPU)."""
     import torch
@@ -303,16 +346,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    reps = Replicas(dist, f"cuda:{local}")
+    barrier = reps.barrier
+    max_over_ranks = reps.max_over_ranks
 
     t_setup = time.perf_counter()
     A, b = problem(M)
@@ -472,8 +508,7 @@ def main():
             "value": 1e3 * t, "unit": "ms", "cores": cores, "kind": kind,
             "sample": f"one full FP64 PCG-IC(0) solve to 1e-10 ({iters} iterations) of the same "
                       f"system; ic_0 factorisation excluded (timed separately: {tf:.3f} s)"}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    reps.emit(line)
     if dist is not None:
         dist.destroy_process_group()
 
