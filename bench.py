@@ -221,7 +221,8 @@ def _local_ms(fn, reps, stream):
 def batched_workload(M, ctx, stream):
     """512 independent random-graph Laplacians (n log-uniform in [1e3, 65536],
     average degree U[8, 32], shift 1e-2 mean degree, seed 3), b ~ N(0,1):
-    one batched PCG to 1e-8 in FP64, Jacobi and IC(0)."""
+    one batched PCG to 1e-8 with Jacobi and IC(0), in FP64 and with FP32 inner
+    solves refined in FP64."""
     systems, (n, rp, ci, v, off) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2, seed=3)
     b = M.normal(n, 3)
     dA = M.Csr(ctx, rp, ci, v)
@@ -241,6 +242,24 @@ def batched_workload(M, ctx, stream):
         rel = max(r.true_resid / r.norm_r0 for r in res[-1])
         out[pc] = {"ms": ms, "iterations_max": int(its.max()),
                    "iterations_mean": float(its.mean()), "max_true_rel_residual": rel}
+        P.close()
+        # FP32 inner solves with FP64 refinement per system
+        P = M.Pc(dA, pc, M.FP32)
+
+        def run32():
+            ctx.xpay(dz, 0.0, dx)
+            st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=5000,
+                                      mode=M.SOLVE_MIXED)
+            assert st == M.OK, st
+            return res
+        run32()
+        ms, res = _local_ms(run32, 2, stream)
+        its = np.array([r.iterations for r in res[-1]])
+        rel = max(r.true_resid / r.norm_r0 for r in res[-1])
+        out[pc + "_fp32_refined"] = {
+            "ms": ms, "inner_iterations_max": int(its.max()),
+            "outer_max": int(max(r.outer_iterations for r in res[-1])),
+            "max_true_rel_residual": rel}
         P.close()
     dA.close()
     return out

@@ -290,9 +290,12 @@ void mtlgpu_iter_params_default(mtlgpu_iter_params* p);
  * (basic_iteration.hpp:31-39): its own scalars, iteration count and stopping
  * test.  P may be NULL (identity) or a diagonal / ic_0 / ilu_0 preconditioner
  * of A (factorising a block-diagonal matrix factorises each block).  Only
- * MTLGPU_CG and FP64 mode.  h_results (host, count entries) receives each
- * system's iteration state; the call returns MTLGPU_MAX_ITER when any system
- * stopped on max_iter. */
+ * MTLGPU_CG.  Mode MTLGPU_SOLVE_MIXED_REFINED runs FP32 inner batched PCG
+ * (preconditioner created with MTLGPU_FP32) inside FP64 iterative refinement
+ * per system, as mtlgpu_solve does for one system; iterations then counts
+ * inner iterations and outer_iterations the refinement steps.  h_results
+ * (host, count entries) receives each system's iteration state; the call
+ * returns MTLGPU_MAX_ITER when any system stopped on max_iter. */
 mtlgpu_status mtlgpu_solve_batched(int method, mtlgpu_csr* A, mtlgpu_pc* P, int count,
                                    const int32_t* h_offsets, double* d_x, const double* d_b,
                                    const mtlgpu_iter_params* params,

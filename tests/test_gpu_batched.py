@@ -58,3 +58,23 @@ def test_batched_max_iter_and_arguments(M, ctx):
     bad[1] += 1
     st, _ = M.solve_batched(dA, None, bad, dx, db)
     assert st == M.INVALID_ARG
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pc", ["diagonal", "ic0"])
+def test_batched_mixed_refinement_reaches_fp64_tolerance(M, ctx, pc):
+    # FP32 inner batched PCG, FP64 refinement per system, to 1e-8 true residual
+    systems, (n, rp, ci, v, off) = M.graph_batch(10, 200, 3000, 8.0, 32.0, 1e-2, seed=5)
+    b = M.normal(n, 6)
+    dA = M.Csr(ctx, rp, ci, v)
+    P = M.Pc(dA, pc, M.FP32)
+    dx, db = ctx.to_device(np.zeros(n)), ctx.to_device(b)
+    st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=4000, mode=M.SOLVE_MIXED)
+    assert st == M.OK
+    x = dx.download()
+    for s, A_s in enumerate(systems):
+        a, e = off[s], off[s + 1]
+        tr = np.linalg.norm(b[a:e] - M.csr_mult(A_s, x[a:e])) / np.linalg.norm(b[a:e])
+        assert res[s].error == 0 and res[s].outer_iterations >= 1
+        assert tr <= 1e-8, (s, tr)
+        assert abs(res[s].true_resid / np.linalg.norm(b[a:e]) - tr) <= 1e-10
