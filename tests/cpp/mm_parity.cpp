@@ -1,0 +1,48 @@
+// Matrix Market: <mtlgpu/matrix_market.hpp> against the reference's own
+// reader (mtl::io::matrix_market_istream, mtl/io/matrix_market.hpp) on the
+// same inputs.  Host-only; built where the MTL4 headers are present.  Prints
+// one JSON line per case with whether both readers give the same CSR arrays.
+#include <boost/numeric/mtl/mtl.hpp>
+
+#include <mtlgpu/matrix_market.hpp>
+
+#include <cstdio>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+const char* kCases[][2] = {
+    {"general", "%%MatrixMarket matrix coordinate real general\n% a comment\n3 4 5\n"
+                "1 1 2.5\n3 4 -1\n2 2 4\n1 3 0.5\n3 1 7\n"},
+    {"symmetric", "%%MatrixMarket matrix coordinate real symmetric\n4 4 6\n1 1 4\n2 1 -1\n"
+                  "2 2 4\n3 2 -1\n4 4 4\n4 1 -0.5\n"},
+    {"skew", "%%MatrixMarket matrix coordinate real skew-symmetric\n3 3 2\n2 1 1.5\n3 2 -2\n"},
+    {"pattern", "%%MatrixMarket matrix coordinate pattern general\n3 3 4\n1 1\n2 3\n3 1\n3 3\n"},
+    {"integer", "%%MatrixMarket matrix coordinate integer symmetric\n3 3 3\n1 1 5\n3 1 -2\n3 3 9\n"},
+    {"duplicate", "%%MatrixMarket matrix coordinate real general\n2 2 3\n1 1 1\n1 1 3\n2 2 5\n"},
+    {"array", "%%MatrixMarket matrix array real general\n2 3\n1\n2\n0\n4\n5\n6\n"},
+};
+
+}  // namespace
+
+int main() {
+  int fails = 0;
+  for (auto& c : kCases) {
+    std::istringstream s1(c[1]), s2(c[1]);
+    mtl::compressed2D<double> R;
+    mtl::io::matrix_market_istream mm(s1);
+    mm >> R;
+    mtlgpu::io::csr_matrix G = mtlgpu::io::read_matrix_market(s2);
+    bool same = int(num_rows(R)) == G.n_rows && int(num_cols(R)) == G.n_cols &&
+                int(R.nnz()) == G.nnz();
+    for (int i = 0; same && i <= G.n_rows; ++i) same = int(R.ref_major()[i]) == G.starts[i];
+    for (int k = 0; same && k < G.nnz(); ++k)
+      same = int(R.ref_minor()[k]) == G.indices[k] && R.data[k] == G.data[k];
+    fails += !same;
+    std::printf("{\"case\": \"%s\", \"same\": %d, \"nnz_ref\": %d, \"nnz\": %d}\n", c[0], int(same),
+                int(R.nnz()), G.nnz());
+  }
+  return fails ? 1 : 0;
+}
