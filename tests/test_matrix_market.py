@@ -72,7 +72,8 @@ def test_solve_matrix_read_from_file(M, ctx, restate, tmp_path):
     n0, rp, ci, v = M.laplacian2d(30, 30)
     rows = np.repeat(np.arange(n0), np.diff(rp))
     low = ci <= rows       # lower triangle, written as a symmetric file
-    text = "%%MatrixMarket matrix coordinate real symmetric\n%d %d %d\n" % (n0, n0, low.sum())
+    text = "%%MatrixMarket matrix coordinate real symmetric\n"
+    text += "{} {} {}\n".format(n0, n0, int(low.sum()))
     text += "".join("%d %d %.17g\n" % (r + 1, c + 1, x)
                     for r, c, x in zip(rows[low], ci[low], v[low]))
     rc, A = read(write(tmp_path, "lap.mtx", text))
