@@ -3,14 +3,23 @@
 Laplacian (n = 2,097,152, nnz = 14,581,760, CSR int32 / float64), PCG with
 IC(0), x_true ~ U[-1,1] (seed 1), b = A x_true, x0 = 0.
 
-One step = one complete mixed-precision refined PCG-IC(0) solve (FP32 inner
-PCG with FP32 factors, FP64 residual / update / stopping norm) to true
-relative residual <= 1e-10, inputs resident in HBM.  Also measured in the
-same run: the plain FP64 GPU solve (for the mixed-vs-FP64 comparison), the
-FP64 SpMV's fraction of the measured HBM peak, the dominant kernel's
-roofline, the same solve end to end through the C ABI with host buffers,
-and the reference's own CPU path (MTL4 compiled from its headers) on the
-host cores.
+One step = one complete mixed-precision refined PCG-IC(0) solve to a true
+relative residual <= 1e-10, inputs resident in HBM: FP32 inner PCG (FP32
+values, FP32 IC(0) factors applied with JACOBI_K Jacobi iterations per
+triangle, FP32 vectors, compensated FP32 dots), FP64 residual, update and
+stopping norm.  Also measured in the same run:
+  * the plain FP64 GPU solve (exact level-scheduled triangular solves, the
+    reference's iteration count) -- the mixed-vs-FP64 comparison -- and, for
+    transparency, the mixed solve with exact sweeps and the FP64 solve with
+    Jacobi-applied factors;
+  * the FP64 SpMV on 128^3 (7-point) and 96^3 (27-point) against the
+    measured HBM peak;
+  * the dominant kernel's roofline;
+  * config 3 (27-point convection-diffusion 96^3, BiCGSTAB + ILU(0), FP64
+    and mixed);
+  * the same mixed solve end to end through the C ABI with host buffers;
+  * the reference's own CPU path (MTL4 compiled from its headers) on the host
+    cores: its OpenMP and serial builds.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -33,8 +42,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "mtl4-mirror_b200", "python"))
 
 N_GRID = 128
+CD_GRID = 96
+JACOBI_K = 1          # Jacobi iterations per triangle in the FP32 inner solves
+INNER_RTOL = 1e-5     # largest reduction asked of one inner solve
 METRIC = "Krylov time to 1e-10 rel residual (mixed vs FP64 GPU); SpMV % HBM peak"
-WORKLOAD = "3-D 7-point Laplacian 128^3, PCG + IC(0), FP32 inner / FP64 refinement, rtol 1e-10"
+WORKLOAD = ("3-D 7-point Laplacian 128^3, PCG + IC(0), FP32 inner (IC(0) applied by "
+            f"{JACOBI_K} Jacobi iteration(s) per triangle) / FP64 refinement, rtol 1e-10")
 
 
 def peaks():
@@ -113,34 +126,53 @@ def problem(M):
     return A, b
 
 
-def reference_solver():
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_solver(flavour="omp"):
     """The reference's own CPU path: MTL4 compiled from its headers
-    (oracle/_ref, OpenMP build, all host threads); the C restatement of it
-    when that build is absent."""
+    (oracle/_ref: 'omp' = the OpenMP build on all host threads, 'serial' = the
+    default build); the C restatement of it when that build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    ref = oracle.available_reference(openmp=True)
+    ref = oracle.available_reference(flavour=flavour)
     if ref is not None:
-        return ref, "reference", ref.threads()
+        return ref, "reference", ref.threads() if flavour == "omp" else 1
     return oracle.Restatement(), "port", 1
 
 
-def time_reference_solve(ref, kind, A, b):
+def reference_problem(M, ref, grid=N_GRID, conv=False):
+    """The workload built for the reference arm without the solver library:
+    the seeded generators of libmtlgpu_fixtures, b = A x_true by the
+    reference's own SpMV."""
+    A = M.convdiff27(grid, 2) if conv else M.laplacian3d(grid)
+    xt = M.uniform(A[0], 1)
+    return A, ref.spmv(A, xt)
+
+
+def time_reference_solve(ref, kind, A, b, method="cg", pc="ic0"):
     t0 = time.perf_counter()
-    r = ref.solve("cg", "ic0", A, b, rtol=1e-10, max_iter=2000)
+    r = ref.solve(method, pc, A, b, rtol=1e-10, max_iter=2000)
     wall = time.perf_counter() - t0
     # the reference driver times the itl::cg call alone (factorisation apart)
     return (r["t_solve"] if kind == "reference" else wall), r["iterations"], r["t_factor"]
 
 
 def run_reference_arm(args, rank):
-    import mtlgpu as M
+    import mtlgpu as M   # seeded generators only (libmtlgpu_fixtures); no solver library
     if rank != 0:
         return
-    A, b = problem(M)
+    ref, kind, cores = reference_solver("omp")
+    A, b = reference_problem(M, ref)
     steps = max(1, args.steps)
     warm = max(0, min(args.warmup, 1))   # one warm-up solve: each step is seconds of CPU work
-    ref, kind, cores = reference_solver()
     for _ in range(warm):
         time_reference_solve(ref, kind, A, b)
     ts, iters = [], None
@@ -156,11 +188,46 @@ def run_reference_arm(args, rank):
                                "reference's CPU path), rtol 1e-10", "n": A[0], "nnz": len(A[2])},
         "iterations": iters,
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": kind,
+                         "cpu_model": cpu_model(),
                          "sample": f"full solve to 1e-10 ({iters} iterations) per step; "
                                    "ic_0 factorisation outside the timed call"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(M, A, b, A3, b3):
+    """The reference's CPU path on the host cores (rank 0, N = 1): the full
+    FP64 PCG-IC(0) solve (median of 3, OpenMP build; 1 run of the serial
+    build), ic_0 factorisation (median of 3), one SpMV (mean over 1000 reps
+    with OpenMP, 100 serial: the sparse_matrix_vector_timing.cpp protocol), and
+    config 3's bicgstab + ilu_0 solve (OpenMP build)."""
+    ref, kind, cores = reference_solver("omp")
+    out = {"unit": "ms", "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+           "nproc": os.cpu_count()}
+    time_reference_solve(ref, kind, A, b)   # warm-up
+    runs = [time_reference_solve(ref, kind, A, b) for _ in range(3)]
+    out["value"] = 1e3 * statistics.median(r[0] for r in runs)
+    out["ic0_factor_ms"] = 1e3 * statistics.median(r[2] for r in runs)
+    iters = runs[-1][1]
+    x = M.uniform(A[0], 5)
+    if kind == "reference":
+        out["spmv_ms_omp"] = 1e3 * ref.spmv_time(A, x, 1000)   # seconds per product
+    ser, skind, _ = reference_solver("serial")
+    if skind == "reference":
+        t, _, tf = time_reference_solve(ser, skind, A, b)
+        out["serial_solve_ms"] = 1e3 * t
+        out["serial_ic0_factor_ms"] = 1e3 * tf
+        out["spmv_ms_serial"] = 1e3 * ser.spmv_time(A, x, 100)
+    t3, it3, tf3 = time_reference_solve(ref, kind, A3, b3, "bicgstab", "ilu0")
+    out["config3_bicgstab_ilu0_ms"] = 1e3 * t3
+    out["config3_ilu0_factor_ms"] = 1e3 * tf3
+    out["config3_iterations"] = it3
+    out["sample"] = (f"full FP64 PCG-IC(0) solves to 1e-10 ({iters} iterations) of the same "
+                     "system, median of 3 after 1 warm-up (OpenMP build, all host threads); "
+                     "factorisation timed separately; SpMV 1000 reps (OpenMP) / 100 reps "
+                     "(serial); config 3: one FP64 bicgstab + ilu_0 solve (OpenMP)")
+    return out
 
 
 class Replicas:
@@ -308,18 +375,38 @@ def adjoint_workload(M, ctx, stream):
 
 
 def profile_case(case, grid, launches):
-    """Runs one kernel of the path a few times on an N^3 Laplacian (for
-    profiler captures): 'spmv' (FP64 y = A x), 'sweep64' / 'sweep32' (IC(0)
-    lower sweep in FP64 / FP32)."""
+    """Runs one kernel (or one solve) of the path a few times on an N^3
+    Laplacian, for profiler captures: 'spmv' (FP64 y = A x, SELL-32),
+    'spmv32' (FP32), 'jacobi32' (FP32 IC(0) apply with JACOBI_K Jacobi
+    iterations per triangle), 'sweep64' / 'sweep32' (exact IC(0) lower sweep),
+    'mixed' (complete mixed solves of the headline configuration, for the
+    launch list)."""
     import mtlgpu as M
     A = M.laplacian3d(grid)
     n = A[0]
     ctx = M.Context(0)
     dA = M.Csr(ctx, *A[1:])
-    if case == "spmv":
-        dx, dy = ctx.to_device(M.uniform(n, 5)), ctx.array(n)
+    if case in ("spmv", "spmv32"):
+        dt = np.float32 if case == "spmv32" else np.float64
+        dx, dy = ctx.to_device(M.uniform(n, 5).astype(dt)), ctx.array(n, dt)
         for _ in range(launches):
-            dA.spmv(dx, dy)
+            (dA.spmv_f32 if case == "spmv32" else dA.spmv)(dx, dy)
+    elif case == "jacobi32":
+        P = M.Pc(dA, "ic0", M.FP32)
+        P.set_jacobi_sweeps(JACOBI_K)
+        r, z = ctx.to_device(np.ones(n, np.float32)), ctx.array(n, np.float32)
+        for _ in range(launches):
+            P.apply_f32(r, z)
+    elif case == "mixed":
+        P = M.Pc(dA, "ic0", M.FP32)
+        P.set_jacobi_sweeps(JACOBI_K)
+        b = M.csr_mult(A, M.uniform(n, 1))
+        dx, db = ctx.array(n), ctx.to_device(b)
+        for _ in range(launches):
+            dx.upload(np.zeros(n))
+            st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=4000,
+                                 mode=M.SOLVE_MIXED, inner_rtol=INNER_RTOL)
+            assert st == M.OK, st
     else:
         prec = M.FP32 if case == "sweep32" else M.FP64
         dt = np.float32 if prec == M.FP32 else np.float64
@@ -339,8 +426,9 @@ def main():
     ap.add_argument("--impl", default="mtlgpu", choices=["mtlgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched and differentiable-solve measurements")
-    ap.add_argument("--profile-case", choices=["spmv", "sweep64", "sweep32"])
+                    help="skip the config-3, batched and differentiable-solve measurements")
+    ap.add_argument("--profile-case",
+                    choices=["spmv", "spmv32", "jacobi32", "sweep64", "sweep32", "mixed"])
     ap.add_argument("--grid", type=int, default=64)
     ap.add_argument("--launches", type=int, default=3)
     args = ap.parse_args()
@@ -381,6 +469,7 @@ def main():
     t_fac64 = time.perf_counter() - t0
     t0 = time.perf_counter()
     P32 = M.Pc(dA, "ic0", M.FP32)
+    P32.set_jacobi_sweeps(JACOBI_K)
     ctx.synchronize()
     t_fac32 = time.perf_counter() - t0
     db = ctx.to_device(b)
@@ -391,34 +480,32 @@ def main():
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    def timed(fn, reps):
-        """Mean ms of fn over reps, CUDA events on the library's stream."""
+    def timed(fn, reps_):
+        """Mean ms of fn over reps_, CUDA events on the library's stream."""
         ctx.synchronize()
         barrier()
         e0, e1 = ev(), ev()
         e0.record(stream)
-        out = [fn() for _ in range(reps)]
+        out = [fn() for _ in range(reps_)]
         e1.record(stream)
         ctx.synchronize()
         torch.cuda.synchronize()
         barrier()
-        return e0.elapsed_time(e1) / reps, out
+        return e0.elapsed_time(e1) / reps_, out
 
-    mixed_kw = dict(rtol=1e-10, max_iter=4000, mode=M.SOLVE_MIXED, inner_rtol=1e-6)
+    mixed_kw = dict(rtol=1e-10, max_iter=4000, mode=M.SOLVE_MIXED, inner_rtol=INNER_RTOL)
     fp64_kw = dict(rtol=1e-10, max_iter=2000)
 
-    def solve_mixed():
-        ctx.xpay(dzero, 0.0, dx)                # x0 = 0 on the device
-        st, res, _ = M.solve("cg", dA, P32, dx, db, **mixed_kw)
-        assert st == M.OK, st
-        return res
+    def solver(P, kw, method="cg", dA_=dA, dx_=dx, db_=db, dzero_=dzero):
+        def run():
+            ctx.xpay(dzero_, 0.0, dx_)                # x0 = 0 on the device
+            st, res, _ = M.solve(method, dA_, P, dx_, db_, **kw)
+            assert st == M.OK, st
+            return res
+        return run
 
-    def solve_fp64():
-        ctx.xpay(dzero, 0.0, dx)
-        st, res, _ = M.solve("cg", dA, P64, dx, db, **fp64_kw)
-        assert st == M.OK, st
-        return res
-
+    solve_mixed = solver(P32, mixed_kw)
+    solve_fp64 = solver(P64, fp64_kw)
     warm = max(3, args.warmup)
     for _ in range(warm):
         solve_mixed()
@@ -436,33 +523,58 @@ def main():
     true_rel = float(np.linalg.norm(b - M.csr_mult(A, x_mixed)) / np.linalg.norm(b))
     launches = int(sum(r.kernel_launches for r in res_mixed))
 
-    # FP64 SpMV alone (matrix 175 MB > L2; y = A x)
-    dy = ctx.array(n)
-    dx.upload(M.uniform(n, 5))
-    for _ in range(5):
-        dA.spmv(dx, dy)
-    ms_spmv, _ = timed(lambda: dA.spmv(dx, dy), 100)
-    bytes_spmv = nnz * 12 + 4 * (n + 1) + 2 * n * 8
-    peak, peak_kind = peaks()
-    spmv_gbs = bytes_spmv / ms_spmv / 1e6
+    # transparency: which part of the gain is the approximate triangular solve
+    P32.set_jacobi_sweeps(0)
+    solve_mixed()
+    ms_mixed_exact, res_mx = timed(solve_mixed, 2)
+    P32.set_jacobi_sweeps(JACOBI_K)
+    P64.set_jacobi_sweeps(JACOBI_K)
+    solve_fp64()
+    ms_fp64_jacobi, res_fj = timed(solve_fp64, 2)
+    P64.set_jacobi_sweeps(0)
 
-    # dominant kernel: the triangular sweep (FP32 in the mixed path).  Each
-    # timed call also refills its output with the NaN-box sentinel (one
-    # extra n*w write, a separate small kernel); achieved counts the
-    # algorithmic bytes of the sweep only.
-    L32 = P32.factor_info(M.LOWER)[0]
+    peak, peak_kind = peaks()
+
+    def spmv_stats(dA_, n_, nnz_, reps_=100):
+        dxs, dys = ctx.to_device(M.uniform(n_, 5)), ctx.array(n_)
+        for _ in range(5):
+            dA_.spmv(dxs, dys)
+        ms, _ = timed(lambda: dA_.spmv(dxs, dys), reps_)
+        byt = nnz_ * 12 + 4 * (n_ + 1) + 2 * n_ * 8
+        return {"ms": ms, "GBps": byt / ms / 1e6, "hbm_frac": byt / ms / 1e6 / peak,
+                "bytes": byt, "peak_kind": peak_kind}
+
+    spmv = spmv_stats(dA, n, nnz)
+
+    # The mixed solve's kernels, timed alone on the same data (FP32): the
+    # Jacobi passes of the IC(0) apply and the FP32 SpMV.  Algorithmic bytes:
+    # a pass reads the factor's off-diagonal entries (4-byte value + 4-byte
+    # index), v, D and the previous iterate once and writes one vector; the
+    # SpMV as above with 4-byte values and vectors.
+    nnz_off = P32.factor_info(M.LOWER)[0] - n
+    bytes_pass = nnz_off * 8 + 4 * (n // 32 + 1) + 4 * n * 4
     r32 = ctx.to_device(np.ones(n, np.float32))
     z32 = ctx.array(n, np.float32)
     for _ in range(3):
-        P32.sweep(M.LOWER, r32, z32)
-    ms_sweep32, _ = timed(lambda: P32.sweep(M.LOWER, r32, z32), 20)
-    bytes_sweep32 = L32 * (4 + 4) + 4 * (n + 1) + 2 * n * 4
+        P32.apply_f32(r32, z32)
+    ms_apply32, _ = timed(lambda: P32.apply_f32(r32, z32), 50)
+    ms_pass = ms_apply32 / (2 * JACOBI_K)
+    x32 = ctx.to_device(M.uniform(n, 5).astype(np.float32))
+    y32 = ctx.array(n, np.float32)
+    for _ in range(5):
+        dA.spmv_f32(x32, y32)
+    ms_spmv32, _ = timed(lambda: dA.spmv_f32(x32, y32), 100)
+    bytes_spmv32 = nnz * 8 + 4 * (n + 1) + 2 * n * 4
+    traffic = read_traffic()
+
+    # exact sweeps (the FP64 path's dominant kernel), for the record
     L64 = P64.factor_info(M.LOWER)[0]
     r64 = ctx.to_device(np.ones(n))
     z64 = ctx.array(n)
+    for _ in range(3):
+        P64.sweep(M.LOWER, r64, z64)
     ms_sweep64, _ = timed(lambda: P64.sweep(M.LOWER, r64, z64), 20)
     bytes_sweep64 = L64 * 12 + 4 * (n + 1) + 2 * n * 8
-    traffic = read_traffic()
 
     # end to end through the C ABI with pinned host buffers, H2D/D2H inside
     hb = torch.from_numpy(b).pin_memory()
@@ -478,6 +590,14 @@ def main():
     ms_e2e, _ = timed(e2e_step, steps)
     ms_e2e = max_over_ranks(ms_e2e)
 
+    dominant = {
+        "jacobi_pass_kernel<float> (IC(0) apply, 1 Jacobi pass)": (ms_pass, bytes_pass,
+                                                                    2 * JACOBI_K,
+                                                                    "jacobi_pass_f32"),
+        "spmv_sell<float,8> (q = A p, FP32)": (ms_spmv32, bytes_spmv32, 1, "spmv_sell_f32"),
+    }
+    dom = max(dominant, key=lambda k: dominant[k][0] * dominant[k][2])
+    d_ms, d_bytes, _, d_key = dominant[dom]
     line = {
         "metric": METRIC,
         "value": ms_mixed,
@@ -492,44 +612,87 @@ def main():
         "dtype": "f32+f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": n, "nnz": nnz, "index": "int32",
+                   "jacobi_iterations_per_triangle": JACOBI_K, "inner_rtol": INNER_RTOL,
                    "l2": "inputs larger than L2 (matrix 175 MB + factors 2 x 100 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "iterations": {"mixed_inner": res_mixed[-1].iterations,
                        "mixed_outer": res_mixed[-1].outer_iterations,
-                       "fp64": res_fp64[-1].iterations},
+                       "fp64": res_fp64[-1].iterations,
+                       "mixed_exact_sweeps_inner": res_mx[-1].iterations,
+                       "fp64_jacobi": res_fj[-1].iterations},
         "true_rel_residual": true_rel,
         "fp64_ms": ms_fp64,
         "mixed_speedup_vs_fp64": ms_fp64 / ms_mixed,
-        "spmv": {"ms": ms_spmv, "GBps": spmv_gbs, "hbm_frac": spmv_gbs / peak,
-                 "bytes": bytes_spmv, "peak_kind": peak_kind},
-        "roofline": {"kernel": "sweep_kernel<float,4> (IC(0) lower sweep, FP32)",
-                     "bound": "hbm", "achieved": bytes_sweep32 / ms_sweep32 / 1e6,
-                     "peak": peak, "unit": "GB/s",
-                     "frac": bytes_sweep32 / ms_sweep32 / 1e6 / peak,
-                     "traffic": traffic.get("sweep_f32_lower"),
-                     "algorithmic_bytes": bytes_sweep32, "ms": ms_sweep32,
-                     "peak_kind": peak_kind},
+        "mixed_exact_sweeps_ms": ms_mixed_exact,
+        "fp64_jacobi_sweeps_ms": ms_fp64_jacobi,
+        "spmv": spmv,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": d_bytes / d_ms / 1e6,
+                     "peak": peak, "unit": "GB/s", "frac": d_bytes / d_ms / 1e6 / peak,
+                     "traffic": traffic.get(d_key), "algorithmic_bytes": d_bytes,
+                     "ms": d_ms, "peak_kind": peak_kind},
+        "mixed_kernels": {"jacobi_pass_f32": {"ms": ms_pass, "GBps": bytes_pass / ms_pass / 1e6,
+                                              "bytes": bytes_pass,
+                                              "launches_per_iteration": 2 * JACOBI_K},
+                          "spmv_f32": {"ms": ms_spmv32, "GBps": bytes_spmv32 / ms_spmv32 / 1e6,
+                                       "bytes": bytes_spmv32}},
         "sweep_fp64": {"ms": ms_sweep64, "GBps": bytes_sweep64 / ms_sweep64 / 1e6,
-                       "bytes": bytes_sweep64},
+                       "bytes": bytes_sweep64, "levels": P64.factor_info(M.LOWER)[1]},
         "setup_s": {"total": setup_s, "ic0_fp64": t_fac64, "ic0_fp32": t_fac32},
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 2 * n * 8,
                 "d2h_bytes_per_step": n * 8},
         "gpu_launches": launches,
         "clocks": clk,
     }
+    A3 = b3 = None
     if world == 1 and not args.no_extras:
+        A3, b3, line["config3"] = config3_workload(M, ctx, timed, solver, spmv_stats, peak)
         line["batched"] = batched_workload(M, ctx, stream)
         line["differentiable_solve"] = adjoint_workload(M, ctx, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ref, kind, cores = reference_solver()
-        t, iters, tf = time_reference_solve(ref, kind, A, b)
-        line["cpu_baseline"] = {
-            "value": 1e3 * t, "unit": "ms", "cores": cores, "kind": kind,
-            "sample": f"one full FP64 PCG-IC(0) solve to 1e-10 ({iters} iterations) of the same "
-                      f"system; ic_0 factorisation excluded (timed separately: {tf:.3f} s)"}
+        if A3 is None:
+            A3 = M.convdiff27(CD_GRID, 2)
+            b3 = M.csr_mult(A3, M.uniform(A3[0], 1))
+        line["cpu_baseline"] = cpu_baseline(M, A, b, A3, b3)
     reps.emit(line)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def config3_workload(M, ctx, timed, solver, spmv_stats, peak):
+    """Config 3: 27-point convection-diffusion on 96^3 (seed 2), x_true ~
+    U[-1,1] (seed 1), b = A x_true; BiCGSTAB + ILU(0) to 1e-10 in FP64 (exact
+    triangular solves: the reference's iteration count) and mixed (FP32
+    inner solve, ILU(0) applied by JACOBI_K Jacobi iterations per triangle,
+    FP64 refinement)."""
+    A = M.convdiff27(CD_GRID, 2)
+    n, nnz = A[0], len(A[2])
+    b = M.csr_mult(A, M.uniform(n, 1))
+    dA = M.Csr(ctx, *A[1:])
+    P64 = M.Pc(dA, "ilu0", M.FP64)
+    P32 = M.Pc(dA, "ilu0", M.FP32)
+    P32.set_jacobi_sweeps(JACOBI_K)
+    db, dx, dz = ctx.to_device(b), ctx.array(n), ctx.to_device(np.zeros(n))
+    kw = dict(dA_=dA, dx_=dx, db_=db, dzero_=dz)
+    fp64 = solver(P64, dict(rtol=1e-10, max_iter=2000), "bicgstab", **kw)
+    mixed = solver(P32, dict(rtol=1e-10, max_iter=4000, mode=M.SOLVE_MIXED,
+                             inner_rtol=INNER_RTOL), "bicgstab", **kw)
+    fp64()
+    mixed()
+    ms_fp64, r64 = timed(fp64, 2)
+    ms_mixed, rmx = timed(mixed, 3)
+    x = dx.download()
+    out = {"workload": "27-point convection-diffusion 96^3, BiCGSTAB + ILU(0), rtol 1e-10",
+           "n": n, "nnz": nnz, "mixed_ms": ms_mixed, "fp64_ms": ms_fp64,
+           "mixed_speedup_vs_fp64": ms_fp64 / ms_mixed,
+           "iterations": {"fp64": r64[-1].iterations, "mixed_inner": rmx[-1].iterations,
+                          "mixed_outer": rmx[-1].outer_iterations},
+           "true_rel_residual": float(np.linalg.norm(b - M.csr_mult(A, x)) / np.linalg.norm(b)),
+           "jacobi_iterations_per_triangle": JACOBI_K,
+           "spmv": spmv_stats(dA, n, nnz)}
+    P32.close()
+    P64.close()
+    dA.close()
+    return A, b, out
 
 
 if __name__ == "__main__":

@@ -141,6 +141,8 @@ mtlgpu_status mtlgpu_ctx_create(int device, mtlgpu_ctx** out);
 /* Use an existing stream (a cudaStream_t passed as void*). */
 mtlgpu_status mtlgpu_ctx_create_on_stream(int device, void* stream, mtlgpu_ctx** out);
 mtlgpu_status mtlgpu_ctx_destroy(mtlgpu_ctx* ctx);
+/* Waits for the context's work; reports (and clears) a device-side error of
+ * it, e.g. a bounded wait of an asynchronous call that ran out. */
 mtlgpu_status mtlgpu_ctx_synchronize(mtlgpu_ctx* ctx);
 void* mtlgpu_ctx_stream(mtlgpu_ctx* ctx);
 /* Upper bound on polls of one bounded device wait before it gives up with
@@ -196,6 +198,10 @@ mtlgpu_status mtlgpu_csr_autotune(mtlgpu_csr* A, int* h_choice);
  * mtl/operation/mat_vec_mult.hpp:620-689).  beta == 0 never reads y. */
 mtlgpu_status mtlgpu_spmv(mtlgpu_csr* A, const double* d_x, double* d_y, double alpha,
                           double beta);
+/* y = A * x with float32 vectors and A's values rounded to float: the SpMV
+ * the inner solves of MIXED_REFINED run (mat_vec_mult.hpp:620-689 on
+ * compressed2D<float>).  Asynchronous on the context's stream. */
+mtlgpu_status mtlgpu_spmv_f32(mtlgpu_csr* A, const float* d_x, float* d_y);
 /* y = A^T x (trans(A) * x; transposed_sparse_matrix_vector_product_test.cpp:32). */
 mtlgpu_status mtlgpu_spmv_transposed(mtlgpu_csr* A, const double* d_x, double* d_y);
 
@@ -244,6 +250,12 @@ mtlgpu_status mtlgpu_pc_destroy(mtlgpu_pc* P);
 mtlgpu_status mtlgpu_pc_apply(mtlgpu_pc* P, const double* d_r, double* d_z);
 /* z = adjoint_solve(P, r) (ilu.hpp:106-115, ic_0.hpp:99-103, diagonal.hpp:75-82) */
 mtlgpu_status mtlgpu_pc_adjoint_apply(mtlgpu_pc* P, const double* d_r, double* d_z);
+/* z = solve(P, r) with float32 vectors and the FP32 factors (preconditioner
+ * created with factor precision MTLGPU_FP32): the apply the inner solves of
+ * MIXED_REFINED run, honouring mtlgpu_pc_set_jacobi_sweeps.  Asynchronous on
+ * the context's stream; a bounded wait that ran out is reported by the next
+ * mtlgpu_ctx_synchronize. */
+mtlgpu_status mtlgpu_pc_apply_f32(mtlgpu_pc* P, const float* d_r, float* d_z);
 /* One triangular sweep: MTLGPU_LOWER is lower_trisolve v5 (ILU, unit
  * diagonal; lower_trisolve.hpp:173-189) or v6 (IC, inverted diagonal last;
  * 192-209); MTLGPU_UPPER is upper_trisolve v3 (inverted diagonal first;
@@ -253,6 +265,28 @@ mtlgpu_status mtlgpu_pc_sweep(mtlgpu_pc* P, int which, const double* d_in, doubl
  * created with factor precision MTLGPU_FP32): the sweep the inner solves of
  * MIXED_REFINED run. */
 mtlgpu_status mtlgpu_pc_sweep_f32(mtlgpu_pc* P, int which, const float* d_in, float* d_out);
+/* Apply the factors of an ic_0 / ilu_0 preconditioner with `iters` Jacobi
+ * iterations per triangle instead of the exact triangular solves of
+ * solve(P, r) (ic_0.hpp:80-87, ilu.hpp:84-91 with lower_trisolve.hpp:173-209
+ * and upper_trisolve.hpp:160-176); iters = 0 (the default) restores the exact
+ * solves.  For a triangle T = N + D^-1 (D the stored inverted diagonal, I for
+ * ILU's unit lower factor) the apply computes w_0 = D v,
+ * w_{m+1} = D (v - N w_m), m < iters.  Each iteration is one fully parallel
+ * pass over the factor; the exact solve is a chain of one step per level.  For
+ * IC(0) the applied operator is P(L)^T P(L), symmetric positive definite, so
+ * CG stays valid.  This is an approximation with no counterpart in the
+ * reference: iteration counts differ from the reference's; MIXED_REFINED
+ * solves still stop on the FP64 true residual.  Affects mtlgpu_pc_apply,
+ * mtlgpu_pc_adjoint_apply (IC(0) only; ILU(0) adjoints return
+ * MTLGPU_NOT_SUPPORTED) and every solve with P; not mtlgpu_pc_sweep.
+ * iters is at most 64. */
+mtlgpu_status mtlgpu_pc_set_jacobi_sweeps(mtlgpu_pc* P, int iters);
+/* Diagnostics (no counterpart in the reference): how the solves of P apply
+ * factor `which` in precision `prec`: *kind = 0 level-ordered sync-free sweep,
+ * 1 partitioned sweep (contexts created with MTLGPU_SWEEP=part, where the
+ * partition fits shared memory), 2 Jacobi iterations
+ * (mtlgpu_pc_set_jacobi_sweeps). */
+mtlgpu_status mtlgpu_pc_sweep_kind(const mtlgpu_pc* P, int which, int prec, int* kind);
 /* Factor sizes and level counts: nnz of the factor as the reference stores it
  * (L of IC(0) includes the diagonal, L of ILU(0) does not). */
 mtlgpu_status mtlgpu_pc_factor_info(const mtlgpu_pc* P, int which, int* nnz, int* n_levels);

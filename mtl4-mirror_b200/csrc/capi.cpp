@@ -88,7 +88,8 @@ void csr_release(Csr* A) {
   dfree(ctx, A->d_v32);
   dfree(ctx, A->d_diag);
   dfree(ctx, A->d_bin_rows);
-  dfree(ctx, A->d_blk);
+  dfree(ctx, A->d_meta);
+  sell_free(ctx, &A->sell);
   dfree(ctx, A->d_trp);
   dfree(ctx, A->d_tci);
   dfree(ctx, A->d_tv);
@@ -179,7 +180,7 @@ mtlgpu_status mtlgpu_ctx_destroy(mtlgpu_ctx* c) {
 mtlgpu_status mtlgpu_ctx_synchronize(mtlgpu_ctx* c) {
   if (!c) return MTLGPU_INVALID_ARG;
   MTLGPU_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
-  return MTLGPU_OK;
+  return take_device_error(c);
 }
 
 void* mtlgpu_ctx_stream(mtlgpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
@@ -239,7 +240,8 @@ static mtlgpu_status csr_create_common(mtlgpu_ctx* c, int n_rows, int n_cols, in
   A->nnz = nnz;
   mtlgpu_status s = MTLGPU_OK;
   if ((s = dalloc(c, &A->d_rp, n_rows + 1)) != MTLGPU_OK ||
-      (s = dalloc(c, &A->d_ci, nnz)) != MTLGPU_OK || (s = dalloc(c, &A->d_v, nnz)) != MTLGPU_OK) {
+      (s = dalloc(c, &A->d_ci, nnz)) != MTLGPU_OK ||
+      (s = dalloc(c, &A->d_v, nnz)) != MTLGPU_OK) {
     csr_release(A);
     delete A;
     return s;
@@ -283,10 +285,17 @@ mtlgpu_status mtlgpu_csr_set_values(mtlgpu_csr* A, const double* h_vals, const d
     MTLGPU_TRY_CUDA(c, cudaMemcpyAsync(A->d_v, h_vals ? h_vals : d_vals, sizeof(double) * A->nnz,
                                        h_vals ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                                        c->stream));
+  // Solver graphs recorded on this matrix captured pointers to the derived
+  // copies below: release them (they are re-recorded on the next solve).
+  release_workspaces(A, nullptr);
   dfree(c, A->d_v32);
   dfree(c, A->d_trp);
   dfree(c, A->d_tci);
   dfree(c, A->d_tv);
+  if (A->spmv_kernel == 2) {
+    dfree(c, A->sell.d_val32);  // rebuilt by the next mixed-precision solve
+    MTLGPU_TRY(sell_refill(c, A->d_rp, A->d_ci, A->d_v, 0, &A->sell));
+  }
   MTLGPU_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
   return MTLGPU_OK;
 }
@@ -324,6 +333,17 @@ mtlgpu_status mtlgpu_spmv(mtlgpu_csr* A, const double* x, double* y, double alph
   a.alpha = alpha;
   a.beta = beta;
   MTLGPU_TRY(spmv_launch<double>(A, x, y, a));
+  return MTLGPU_OK;
+}
+
+mtlgpu_status mtlgpu_spmv_f32(mtlgpu_csr* A, const float* x, float* y) {
+  if (!A || (A->n_rows && (!x || !y)) || x == y) return MTLGPU_INVALID_ARG;
+  MTLGPU_TRY(csr_ensure_fp32(A));
+  SpmvArgs a;
+  a.epi = EPI_AXPBY;
+  a.alpha = 1.0;
+  a.beta = 0.0;
+  MTLGPU_TRY(spmv_launch<float>(A, x, y, a));
   return MTLGPU_OK;
 }
 
@@ -405,6 +425,13 @@ mtlgpu_status mtlgpu_pc_adjoint_apply(mtlgpu_pc* P, const double* r, double* z) 
   return pc_apply_common(P, r, z, true);
 }
 
+mtlgpu_status mtlgpu_pc_apply_f32(mtlgpu_pc* P, const float* r, float* z) {
+  if (!P || (P->n && (!r || !z)) || (r == z && P->n) ||
+      (P->prec != MTLGPU_FP32 && P->kind != MTLGPU_PC_IDENTITY))
+    return MTLGPU_INVALID_ARG;
+  return pc_apply_t<float>(P, r, z, false, nullptr, false, false);
+}
+
 mtlgpu_status mtlgpu_pc_sweep(mtlgpu_pc* P, int which, const double* in, double* out) {
   if (!P || (P->kind != MTLGPU_PC_IC0 && P->kind != MTLGPU_PC_ILU0) || in == out)
     return MTLGPU_INVALID_ARG;
@@ -420,6 +447,26 @@ mtlgpu_status mtlgpu_pc_sweep_f32(mtlgpu_pc* P, int which, const float* in, floa
   const SweepPlan& S = which == MTLGPU_LOWER ? P->lower : P->upper;
   MTLGPU_TRY(sweep_launch<float>(P->A->ctx, S, in, out, false, nullptr));
   return take_device_error(P->A->ctx);
+}
+
+mtlgpu_status mtlgpu_pc_set_jacobi_sweeps(mtlgpu_pc* P, int iters) {
+  if (!P || iters < 0 || iters > 64) return MTLGPU_INVALID_ARG;
+  if (iters == P->jacobi_iters) return MTLGPU_OK;
+  // solver graphs recorded with the other kind of apply are stale
+  release_workspaces(P->A, P);
+  MTLGPU_TRY(pc_set_jacobi(P, iters));
+  return take_device_error(P->A->ctx);
+}
+
+mtlgpu_status mtlgpu_pc_sweep_kind(const mtlgpu_pc* P, int which, int prec, int* kind) {
+  if (!P || !kind || (P->kind != MTLGPU_PC_IC0 && P->kind != MTLGPU_PC_ILU0)) return MTLGPU_INVALID_ARG;
+  const SweepPlan& S = which == MTLGPU_LOWER ? P->lower : P->upper;
+  const int pi = prec == MTLGPU_FP32 ? 1 : 0;
+  if (P->jacobi_iters > 0)
+    *kind = 2;
+  else
+    *kind = (S.part && S.part->prec[pi].ready) ? 1 : 0;
+  return MTLGPU_OK;
 }
 
 mtlgpu_status mtlgpu_pc_factor_info(const mtlgpu_pc* P, int which, int* nnz, int* n_levels) {

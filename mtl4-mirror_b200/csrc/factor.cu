@@ -55,6 +55,21 @@ __global__ void jacobi_kernel(int n, const int32_t* __restrict__ diag,
   }
 }
 
+// Reverses the entries of every row in place.
+__global__ void reverse_rows_kernel(int n, const int32_t* __restrict__ rp, int32_t* ci,
+                                    double* v) {
+  for (long long r = gtid(); r < n; r += gstride()) {
+    for (int a = rp[r], b = rp[r + 1] - 1; a < b; a++, b--) {
+      const int32_t tc = ci[a];
+      ci[a] = ci[b];
+      ci[b] = tc;
+      const double tv = v[a];
+      v[a] = v[b];
+      v[b] = tv;
+    }
+  }
+}
+
 __global__ void check_diag_kernel(int n, const int32_t* __restrict__ diag, int* err) {
   for (long long i = gtid(); i < n; i += gstride())
     if (diag[i] < 0) atomicCAS(err, 0, (int)MTLGPU_MISSING_DIAGONAL);
@@ -513,6 +528,12 @@ mtlgpu_status pc_ensure_adjoint(Pc* P) {
   MTLGPU_TRY(dalloc(ctx, &tci, P->nnz_L));
   MTLGPU_TRY(dalloc(ctx, &tv, P->nnz_L));
   MTLGPU_TRY(csr_transpose(ctx, n, n, P->nnz_L, P->d_Lrp, P->d_Lci, P->d_Lv, trp, tci, tv));
+  // The reference applies L^T column by column from the last column down
+  // (upper_trisolve on the adjoint view, column-major: w[j] -= L[r][j] w[r]
+  // for r descending), so each row of L^T takes its entries in descending
+  // column order.
+  if (n)
+    reverse_rows_kernel<<<grid_cap(ctx, n), kBlock, 0, ctx->stream>>>(n, trp, tci, tv);
   MTLGPU_TRY(build_sweep_plan(ctx, n, trp, tci, tv, false, true, false, &P->adj_upper));
   MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   dfree(ctx, trp);
@@ -545,6 +566,33 @@ void pc_release(Pc* P) {
   free_sweep_plan(ctx, &P->upper);
   free_sweep_plan(ctx, &P->adj_lower);
   free_sweep_plan(ctx, &P->adj_upper);
+  sell_free(ctx, &P->jac_lower);
+  sell_free(ctx, &P->jac_upper);
+  dfree(ctx, P->d_jtmp);
+  dfree(ctx, P->d_jtmp32);
+}
+
+// Switches the triangular solves of P between the exact sweeps (iters = 0)
+// and `iters` Jacobi iterations per triangle, building the SELL-32 copies of
+// the factors on first use.  The factors are the reference-layout ones: IC(0)
+// L has its inverted diagonal last, U first; ILU(0) L has a unit diagonal.
+mtlgpu_status pc_set_jacobi(Pc* P, int iters) {
+  if (iters < 0) return MTLGPU_INVALID_ARG;
+  if (P->kind != MTLGPU_PC_IC0 && P->kind != MTLGPU_PC_ILU0) return iters ? MTLGPU_INVALID_ARG : MTLGPU_OK;
+  Ctx* ctx = P->A->ctx;
+  if (iters > 0 && !P->jac_lower.d_slice_ptr && P->n > 0) {
+    const bool f32 = P->prec == MTLGPU_FP32;
+    const int lower_diag = P->kind == MTLGPU_PC_IC0 ? 2 : 0;
+    MTLGPU_TRY(sell_build(ctx, P->n, P->d_Lrp, P->d_Lci, P->d_Lv, lower_diag, true, f32, f32,
+                          &P->jac_lower));
+    MTLGPU_TRY(sell_build(ctx, P->n, P->d_Urp, P->d_Uci, P->d_Uv, 1, true, f32, f32,
+                          &P->jac_upper));
+    MTLGPU_TRY(dalloc(ctx, &P->d_jtmp, P->n));
+    if (f32) MTLGPU_TRY(dalloc(ctx, &P->d_jtmp32, P->n));
+    MTLGPU_TRY(take_device_error(ctx));
+  }
+  P->jacobi_iters = iters;
+  return MTLGPU_OK;
 }
 
 template <typename T>
@@ -552,17 +600,19 @@ struct PcVec;
 template <>
 struct PcVec<double> {
   static double* tmp(Pc* P) { return P->d_tmp; }
+  static double* jtmp(Pc* P) { return P->d_jtmp; }
   static const double* inv(Pc* P) { return P->d_inv_diag; }
 };
 template <>
 struct PcVec<float> {
   static float* tmp(Pc* P) { return P->d_tmp32; }
+  static float* jtmp(Pc* P) { return P->d_jtmp32; }
   static const float* inv(Pc* P) { return P->d_inv_diag32; }
 };
 
 template <typename T>
 mtlgpu_status pc_apply_t(Pc* P, const T* r, T* z, bool adjoint, const int* skip,
-                         bool prefilled_tmp, bool prefilled_out) {
+                         bool prefilled_tmp, bool prefilled_out, double* rho_out) {
   Ctx* ctx = P->A->ctx;
   const int n = P->n;
   if (n == 0) return MTLGPU_OK;
@@ -579,6 +629,16 @@ mtlgpu_status pc_apply_t(Pc* P, const T* r, T* z, bool adjoint, const int* skip,
     default: {
       T* tmp = PcVec<T>::tmp(P);
       if (!tmp) return MTLGPU_INVALID_ARG;
+      if (P->jacobi_iters > 0) {
+        // IC(0): the adjoint solve is the solve itself (U = trans(L)).
+        if (adjoint && P->kind == MTLGPU_PC_ILU0) return MTLGPU_NOT_SUPPORTED;
+        T* scratch = PcVec<T>::jtmp(P);
+        if (!scratch) return MTLGPU_INVALID_ARG;
+        MTLGPU_TRY(jacobi_solve<T>(ctx, P->jac_lower, P->jacobi_iters, r, tmp, scratch, skip));
+        MTLGPU_TRY(jacobi_solve<T>(ctx, P->jac_upper, P->jacobi_iters, tmp, z, scratch, skip,
+                                   rho_out ? r : nullptr, rho_out));
+        break;
+      }
       if (adjoint && P->kind == MTLGPU_PC_ILU0) {
         MTLGPU_TRY(pc_ensure_adjoint(P));
         MTLGPU_TRY(sweep_launch<T>(ctx, P->adj_lower, r, tmp, prefilled_tmp, skip));
@@ -594,7 +654,8 @@ mtlgpu_status pc_apply_t(Pc* P, const T* r, T* z, bool adjoint, const int* skip,
 }
 
 template mtlgpu_status pc_apply_t<double>(Pc*, const double*, double*, bool, const int*, bool,
-                                          bool);
-template mtlgpu_status pc_apply_t<float>(Pc*, const float*, float*, bool, const int*, bool, bool);
+                                          bool, double*);
+template mtlgpu_status pc_apply_t<float>(Pc*, const float*, float*, bool, const int*, bool, bool,
+                                         double*);
 
 }  // namespace mtlgpu

@@ -51,6 +51,23 @@ struct SpmvBin {
   int begin, count; // slice of the bin row list
 };
 
+// SELL-32 copy of a CSR matrix or of a factor's off-diagonal part (sell.cu):
+// slices of 32 rows, entries column-major inside a slice, padding column -1;
+// the stored (inverted) diagonal of a factor separately.
+struct Sell {
+  int n = 0, n_slices = 0;
+  long long n_ent = 0;             // padded entries
+  int max_width = 0;               // largest slice width (entries per row)
+  bool unit_diag = false;
+  bool round64 = false;            // double copy holds float-rounded values
+  int32_t* d_slice_ptr = nullptr;  // n_slices + 1 entry offsets (multiples of 32)
+  int32_t* d_col = nullptr;
+  double* d_val = nullptr;
+  float* d_val32 = nullptr;
+  double* d_dinv = nullptr;
+  float* d_dinv32 = nullptr;
+};
+
 struct Pc;
 // Solver workspace cache entry (buffers + instantiated graph; krylov.cu).
 struct WorkspaceEntry {
@@ -76,11 +93,12 @@ struct Csr {
   int32_t* d_bin_rows = nullptr;   // rows ordered by bin (when !uniform)
   std::vector<SpmvBin> bins;
   int tuned_rows_per_group = 1;    // autotuner choice (1 or 2 rows per pass)
-  // CSR-stream row blocks: block b = rows [blk[b], blk[b+1]), <= 32 rows and
-  // <= 32*8 entries, or a single longer row
-  int32_t* d_blk = nullptr;
+  // CSR-stream row blocks: block b = rows [meta[b].x, meta[b+1].x), entries
+  // [meta[b].y, meta[b+1].y); <= 32 rows and <= 256 entries, or one longer row
+  int2* d_meta = nullptr;
   int n_blk = 0;
-  int spmv_kernel = 0;             // 0 = CSR-stream (default), 1 = row-binned groups
+  int spmv_kernel = 0;             // 0 = CSR-stream, 1 = row-binned groups, 2 = SELL-32
+  Sell sell;                       // SELL-32 copy (spmv_kernel == 2)
   // transpose (built on demand for A^T x)
   int32_t* d_trp = nullptr;
   int32_t* d_tci = nullptr;
@@ -143,6 +161,11 @@ struct Pc {
   double* d_tmp = nullptr;         // y0 of solve_lower (per handle, never static)
   float* d_tmp32 = nullptr;
   int factor_status = MTLGPU_OK;
+  // Triangular solves as Jacobi iterations (0: exact sweeps).
+  int jacobi_iters = 0;
+  Sell jac_lower, jac_upper;
+  double* d_jtmp = nullptr;
+  float* d_jtmp32 = nullptr;
 };
 
 // ---- error plumbing ------------------------------------------------------
@@ -218,6 +241,26 @@ template <typename T>
 mtlgpu_status part_sweep_launch(Ctx* ctx, const SweepPlan& S, const T* in, T* out,
                                 const int* skip);
 
+// SELL-32 layouts (sell.cu).  diag_pos: 0 = every entry kept (a matrix, or
+// a unit-diagonal factor), 1 = the first entry of each row is the diagonal,
+// 2 = the last one; the diagonal then goes to d_dinv.
+long long sell_padded_entries(int n, const int32_t* h_rp, int diag_pos);
+mtlgpu_status sell_build(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_ci,
+                         const double* d_v, int diag_pos, bool fp64, bool fp32, bool round64,
+                         Sell* J);
+mtlgpu_status sell_refill(Ctx* ctx, const int32_t* d_rp, const int32_t* d_ci, const double* d_v,
+                          int diag_pos, Sell* J);
+mtlgpu_status sell_ensure_fp32(Ctx* ctx, const int32_t* d_rp, const int32_t* d_ci,
+                               const double* d_v, int diag_pos, Sell* J);
+void sell_free(Ctx* ctx, Sell* J);
+
+// Jacobi-iteration triangular solves (jacobi_sweep.cu).
+template <typename T>
+mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T* scratch,
+                           const int* skip, const T* dot_with = nullptr,
+                           double* dot_out = nullptr);
+mtlgpu_status pc_set_jacobi(Pc* P, int iters);
+
 // Analysis (analysis.cu)
 mtlgpu_status build_sweep_plan(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_ci,
                                const double* d_v, bool lower, bool unit_diag, bool diag_last,
@@ -237,7 +280,7 @@ void pc_release(Pc* P);
 mtlgpu_status pc_ensure_adjoint(Pc* P);
 template <typename T>
 mtlgpu_status pc_apply_t(Pc* P, const T* r, T* z, bool adjoint, const int* skip,
-                         bool prefilled_tmp, bool prefilled_out);
+                         bool prefilled_tmp, bool prefilled_out, double* rho_out = nullptr);
 
 // BLAS-1 (blas1.cu): results land in device scalar slots.
 mtlgpu_status dot_launch(Ctx* ctx, int n, const double* x, const double* y, double* d_out,

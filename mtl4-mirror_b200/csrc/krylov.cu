@@ -385,7 +385,11 @@ double* pc_tmp<double>(Pc* P) { return P ? P->d_tmp : nullptr; }
 template <>
 float* pc_tmp<float>(Pc* P) { return P ? P->d_tmp32 : nullptr; }
 
-bool uses_sweeps(Pc* P) { return P && (P->kind == MTLGPU_PC_IC0 || P->kind == MTLGPU_PC_ILU0); }
+// Exact sweeps read NaN-boxed outputs that the previous kernel prefilled;
+// Jacobi-iteration solves need no prefill.
+bool uses_sweeps(Pc* P) {
+  return P && (P->kind == MTLGPU_PC_IC0 || P->kind == MTLGPU_PC_ILU0) && P->jacobi_iters == 0;
+}
 
 template <typename T>
 __global__ void copy_if_kernel(int n, const T* __restrict__ a, T* __restrict__ b, const int* skip) {
@@ -416,9 +420,14 @@ mtlgpu_status record_cg_iteration(Workspace<T>* W) {
   if (!ident) {
     zvec = W->z;
     const bool sw = uses_sweeps(W->P);
-    MTLGPU_TRY(pc_apply_t<T>(W->P, W->r, W->z, false, skip, sw, sw));
-    cg_rho_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->z, W->st, ctx->d_partials,
-                                                       counter_slot(ctx, 1));
+    if (W->P->jacobi_iters > 0 && (W->P->kind == MTLGPU_PC_IC0 || W->P->kind == MTLGPU_PC_ILU0)) {
+      // rho = r . z fused into the last Jacobi pass
+      MTLGPU_TRY(pc_apply_t<T>(W->P, W->r, W->z, false, skip, false, false, &W->st->rho));
+    } else {
+      MTLGPU_TRY(pc_apply_t<T>(W->P, W->r, W->z, false, skip, sw, sw));
+      cg_rho_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->z, W->st, ctx->d_partials,
+                                                         counter_slot(ctx, 1));
+    }
   }
   cg_p_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, zvec, W->p, W->st);
   SpmvArgs a;

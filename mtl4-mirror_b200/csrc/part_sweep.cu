@@ -48,6 +48,7 @@
 
 #include "device.cuh"
 #include "internal.h"
+#include "tma.cuh"
 
 namespace mtlgpu {
 
@@ -110,73 +111,6 @@ __host__ __device__ __forceinline__ int slot_need(const RecHdr& h, int ts) {
   return h.bytes + a16(ts * h.nrows) + 16 * h.next;
 }
 
-template <int N>
-__device__ __forceinline__ void cp_async_ca(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(N) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// mbarrier helpers (shared::cta, 64-bit barrier objects).
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
-  asm volatile(
-      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b))
-      : "memory");
-}
-// Arrives on b expecting `bytes` of asynchronous copies to complete on it.
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* b, unsigned bytes) {
-  asm volatile(
-      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
-          smem_u32(b)),
-      "r"(bytes)
-      : "memory");
-}
-// Bulk copy global -> this CTA's shared memory (TMA, no multicast), completing
-// its bytes on mbarrier b.
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes,
-                                              unsigned long long* b) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(b))
-      : "memory");
-}
-// Arrives on b once every cp.async this thread issued before has completed.
-__device__ __forceinline__ void mbar_arrive_cp_async(unsigned long long* b) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait for the phase with the given parity; false after `limit` polls.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, long long limit) {
-  for (long long k = 0; k < limit; ++k)
-    if (mbar_test(b, parity)) return true;
-  return false;
-}
 __device__ __forceinline__ void consumer_sync() {  // the kPartThreads consumer threads only
   asm volatile("bar.sync 1, %0;" ::"n"(kPartThreads) : "memory");
 }
@@ -222,6 +156,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
     // ---- producer warps: records kRing blocks ahead of the consumers, the
     // gathers of a block kAhead loop steps after its record
     const int pt = tid - kPartThreads;
+    int last_rec = -1;  // pt 0: last record whose bulk copy was issued
     for (int k = 0; k < nb + kAhead; ++k) {
       if (k < nb) {
         if (k >= kRing && !mbar_wait(&empty[k % kRing], ((k / kRing) - 1) & 1, limit)) {
@@ -233,6 +168,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
           const unsigned bytes = (unsigned)(offs[k + 1] - offs[k]) * 16u;
           mbar_arrive_expect_tx(&rec_full[k % kRing], bytes);
           bulk_copy_g2s(slot(k), recs + (size_t)offs[k] * 16, bytes, &rec_full[k % kRing]);
+          last_rec = k;
         }
       }
       const int j = k - kAhead;
@@ -261,6 +197,17 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
         }
         mbar_arrive_cp_async(&full[j % kRing]);
       }
+    }
+    // After an abort, record copies may still be in flight into this CTA's
+    // shared memory: the issuing thread waits for the last phase of every
+    // slot it filled before leaving (shared memory stays valid while any
+    // thread of the CTA runs).  On a normal exit those phases have completed
+    // and each wait returns at once.  A global -> shared bulk copy always
+    // completes; the wait is still bounded, by at least 2^24 polls.
+    if (pt == 0) {
+      const long long drain = limit > (1ll << 24) ? limit : (1ll << 24);
+      for (int k = last_rec - kRing + 1 > 0 ? last_rec - kRing + 1 : 0; k <= last_rec; ++k)
+        mbar_wait(&rec_full[k % kRing], (unsigned)(k / kRing) & 1u, drain);
     }
     cp_async_wait<0>();
     return;

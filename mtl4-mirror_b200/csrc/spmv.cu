@@ -16,9 +16,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 #include "device.cuh"
 #include "internal.h"
+#include "tma.cuh"
 
 namespace mtlgpu {
 
@@ -27,7 +30,8 @@ using namespace dev;
 namespace {
 
 constexpr int kBlock = 256;
-constexpr int kStreamK = 8;  // entries per lane per row block (CSR-stream)
+constexpr int kStreamK = 8;            // entries per lane per row block (CSR-stream)
+constexpr double kSellMaxPadding = 1.2;  // SELL-32 when padded entries <= 1.2 nnz
 
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
@@ -202,20 +206,26 @@ __global__ void __launch_bounds__(kBlock) spmv_cta(int nrows, const int32_t* __r
   finish_epilogue(ep, acc);
 }
 
-// CSR-stream: one warp per row block (<= 32 rows, <= 32*K entries).  Lane l
-// loads entries e0 + l + 32k (k < K): K independent coalesced loads of values
-// and indices, then K gathers of x, all in flight at once; the products are
-// staged in shared memory and lane l sums row r0 + l in column order.  The
-// products and the running sum round separately (no FMA), so every row sum
-// equals the reference's `tmp += A.data[j] * v[A.ref_minor()[j]]`
-// (mat_vec_mult.hpp:666-688) bit for bit.  A block holding a single row
-// longer than 32*K entries is summed by the whole warp instead.
+// CSR-stream: one warp per row block (<= 32 rows, <= 32*K entries), for
+// matrices whose rows are too uneven for SELL-32.  meta[b] = (first row,
+// first entry) of block b, meta[n_blocks] = (n, nnz).  Lane l loads entries
+// e0 + l + 32k (k < K): K coalesced loads of values and column indices
+// (last-use hint: they are streamed once, and x keeps its place in L2), then
+// K gathers of x, all in flight at once, while the row bounds of its row and
+// the next block's metadata are on their way.  The products are staged in
+// shared memory and lane l sums row r0 + l in column order, product and sum
+// rounded separately: every row sum equals the reference's
+// `tmp += A.data[j] * v[A.ref_minor()[j]]` (mat_vec_mult.hpp:666-688) bit for
+// bit.  A block holding a single row longer than 32*K entries is summed by
+// the whole warp instead (tree order).  Registers stay at 32 so that 8 CTAs
+// (64 warps) fit an SM: on B200 every variant with more state per lane and
+// fewer warps measured slower.
 template <typename T, int K>
-__global__ void __launch_bounds__(kBlock)
-    spmv_stream(int n_blocks, const int32_t* __restrict__ blk, const int32_t* __restrict__ rp,
+__global__ void __launch_bounds__(kBlock, 8)
+    spmv_stream(int n_blocks, const int2* __restrict__ meta, const int32_t* __restrict__ rp,
                 const int32_t* __restrict__ ci, const T* __restrict__ val,
                 const T* __restrict__ x, T* __restrict__ y, EpiParams<T> ep) {
-  if (ep.skip && *ep.skip) return;
+  if (ep.skip && ld_relaxed(ep.skip)) return;
   typedef typename AccOf<T, 1>::type R;
   __shared__ T prod[kBlock / 32][32 * K];
   R acc = R::zero();
@@ -223,9 +233,17 @@ __global__ void __launch_bounds__(kBlock)
   T* pw = prod[wib];
   const int warp = (blockIdx.x * kBlock + threadIdx.x) >> 5;
   const int W = (gridDim.x * kBlock) >> 5;
+  int2 ma = make_int2(0, 0), mb = ma;
+  if (warp < n_blocks) {
+    ma = __ldg(meta + warp);
+    mb = __ldg(meta + warp + 1);
+  }
   for (int b = warp; b < n_blocks; b += W) {
-    const int r0 = blk[b], r1 = blk[b + 1];
-    const int e0 = rp[r0], e1 = rp[r1];
+    const int r0 = ma.x, e0 = ma.y, r1 = mb.x, e1 = mb.y;
+    if (b + W < n_blocks) {
+      ma = __ldg(meta + b + W);
+      mb = __ldg(meta + b + W + 1);
+    }
     if (e1 - e0 > 32 * K) {  // a single long row
       T s = T(0);
       for (int j = e0 + lane; j < e1; j += 32) s = s + val[j] * __ldg(x + ci[j]);
@@ -239,8 +257,14 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
     for (int k = 0; k < K; k++) {
       const int j = e0 + k * 32 + lane;
-      c[k] = j < e1 ? ci[j] : 0;
-      v[k] = j < e1 ? val[j] : T(0);
+      c[k] = j < e1 ? __ldlu(ci + j) : 0;
+      v[k] = j < e1 ? __ldlu(val + j) : T(0);
+    }
+    const int row = r0 + lane;
+    int rb = 0, re = 0;
+    if (row < r1) {
+      rb = __ldg(rp + row) - e0;
+      re = __ldg(rp + row + 1) - e0;
     }
 #pragma unroll
     for (int k = 0; k < K; k++) {
@@ -248,14 +272,55 @@ __global__ void __launch_bounds__(kBlock)
       if (j < e1) pw[k * 32 + lane] = mul_rn(v[k], __ldg(x + c[k]));
     }
     __syncwarp();
-    if (lane < r1 - r0) {
-      const int row = r0 + lane;
-      const int b0 = rp[row] - e0, b1 = rp[row + 1] - e0;
+    if (row < r1) {
       T s = T(0);
-      for (int j = b0; j < b1; j++) s = add_rn(s, pw[j]);
+      for (int j = rb; j < re; j++) s = add_rn(s, pw[j]);
       row_epilogue(ep, row, s, y, acc);
     }
     __syncwarp();
+  }
+  finish_epilogue(ep, acc);
+}
+
+// SELL-32 SpMV (sell.cu layout): thread per row, a warp per slice.  Entries
+// are taken in chunks of C: C coalesced loads of column indices and values
+// (last-use hint), then C gathers of x -- for a stencil matrix the k-th
+// gathers of a warp hit 32 consecutive rows' k-th neighbours, so they
+// coalesce as well -- then the row sum continues in stored (column) order,
+// product and sum rounded separately: bit for bit the reference's row loop
+// (mat_vec_mult.hpp:666-688).  Padding (column -1) is skipped.
+template <typename T, int C>
+__global__ void __launch_bounds__(kBlock, 8)
+    spmv_sell(int n, const int32_t* __restrict__ slice_ptr, const int32_t* __restrict__ col,
+              const T* __restrict__ val, const T* __restrict__ x, T* __restrict__ y,
+              EpiParams<T> ep) {
+  if (ep.skip && ld_relaxed(ep.skip)) return;
+  typedef typename AccOf<T, 1>::type R;
+  R acc = R::zero();
+  for (long long r = gtid(); r < n; r += gstride()) {
+    const long long s = r >> 5;
+    const int lane = (int)(r & 31);
+    const int base = __ldg(slice_ptr + s);
+    const int width = (__ldg(slice_ptr + s + 1) - base) >> 5;
+    const int32_t* cp = col + base + lane;
+    const T* vp = val + base + lane;
+    T sum = T(0);
+    for (int k0 = 0; k0 < width; k0 += C) {
+      int c[C];
+      T a[C], xv[C];
+#pragma unroll
+      for (int u = 0; u < C; u++) {
+        const bool in = k0 + u < width;
+        c[u] = in ? __ldlu(cp + 32 * (k0 + u)) : -1;
+        a[u] = in ? __ldlu(vp + 32 * (k0 + u)) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < C; u++) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < C; u++)
+        if (c[u] >= 0) sum = add_rn(sum, mul_rn(a[u], xv[u]));
+    }
+    row_epilogue(ep, (int)r, sum, y, acc);
   }
   finish_epilogue(ep, acc);
 }
@@ -307,19 +372,32 @@ mtlgpu_status csr_analyse(Csr* A) {
   A->max_row = (int)h_stats[0];
   A->mean_row = A->n_rows ? double(h_stats[1]) / A->n_rows : 0.0;
 
-  // CSR-stream row blocks (greedy: up to 32 rows and 32*kStreamK entries; a
-  // longer row forms a block of its own)
+  // SpMV layout.  SELL-32 where its padding is small (stencils: < 1 %);
+  // otherwise CSR-stream row blocks (greedy: up to 32 rows and 32*kStreamK
+  // entries; a longer row forms a block of its own).
   {
     std::vector<int32_t> h_rp(A->n_rows + 1);
     MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h_rp.data(), A->d_rp, sizeof(int32_t) * (A->n_rows + 1),
                                          cudaMemcpyDeviceToHost, ctx->stream));
     MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    std::vector<int32_t> blk;
+    const long long padded = sell_padded_entries(A->n_rows, h_rp.data(), 0);
+    A->spmv_kernel = (A->nnz > 0 && padded <= (long long)(kSellMaxPadding * A->nnz) &&
+                      padded < (1ll << 31))
+                         ? 2
+                         : 0;
+    if (const char* m = std::getenv("MTLGPU_SPMV")) {
+      if (!std::strcmp(m, "stream")) A->spmv_kernel = 0;
+      if (!std::strcmp(m, "group")) A->spmv_kernel = 1;
+    }
+    if (A->spmv_kernel == 2)
+      MTLGPU_TRY(sell_build(ctx, A->n_rows, A->d_rp, A->d_ci, A->d_v, 0, true, false, false,
+                            &A->sell));
+    const int cap = 32 * kStreamK;
+    std::vector<int2> blk;
     blk.reserve(A->n_rows / 16 + 2);
     int r = 0;
-    const int cap = 32 * kStreamK;
     while (r < A->n_rows) {
-      blk.push_back(r);
+      blk.push_back(make_int2(r, h_rp[r]));
       int rows = 0, cnt = 0;
       while (r < A->n_rows && rows < 32) {
         const int len = h_rp[r + 1] - h_rp[r];
@@ -330,10 +408,10 @@ mtlgpu_status csr_analyse(Csr* A) {
         if (cnt > cap) break;
       }
     }
-    blk.push_back(A->n_rows);
+    blk.push_back(make_int2(A->n_rows, A->nnz));
     A->n_blk = (int)blk.size() - 1;
-    MTLGPU_TRY(dalloc(ctx, &A->d_blk, blk.size()));
-    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(A->d_blk, blk.data(), sizeof(int32_t) * blk.size(),
+    MTLGPU_TRY(dalloc(ctx, &A->d_meta, blk.size()));
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(A->d_meta, blk.data(), sizeof(int2) * blk.size(),
                                          cudaMemcpyHostToDevice, ctx->stream));
     MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
@@ -397,8 +475,17 @@ mtlgpu_status csr_ensure_fp32(Csr* A) {
   to_fp32_kernel<<<grid_for(ctx, kBlock, A->nnz), kBlock, 0, ctx->stream>>>(A->nnz, A->d_v,
                                                                             A->d_v32);
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  if (A->spmv_kernel == 2)
+    MTLGPU_TRY(sell_ensure_fp32(ctx, A->d_rp, A->d_ci, A->d_v, 0, &A->sell));
   return MTLGPU_OK;
 }
+
+template <typename T>
+const T* csr_sell_values(Csr* A);
+template <>
+const double* csr_sell_values<double>(Csr* A) { return A->sell.d_val; }
+template <>
+const float* csr_sell_values<float>(Csr* A) { return A->sell.d_val32; }
 
 template <typename T>
 const T* csr_values(Csr* A);
@@ -423,12 +510,25 @@ mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args) {
   ep.skip = args.skip;
   ep.partials = ctx->d_partials;
   ep.counter = counter_slot(ctx, 0);
+  if (A->spmv_kernel == 2) {
+    const T* sv = csr_sell_values<T>(A);
+    if (!sv) return MTLGPU_INVALID_ARG;
+    const int grid = grid_for(ctx, kBlock, A->n_rows);
+    ep.part_off = 0;
+    ep.part_total = grid;
+    ep.final_launch = true;
+    spmv_sell<T, 8><<<grid, kBlock, 0, ctx->stream>>>(A->n_rows, A->sell.d_slice_ptr,
+                                                      A->sell.d_col, sv, x, y, ep);
+    ctx->launches++;
+    MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+    return MTLGPU_OK;
+  }
   if (A->spmv_kernel == 0) {
     int grid = grid_for(ctx, kBlock / 32, A->n_blk);
     ep.part_off = 0;
     ep.part_total = grid;
     ep.final_launch = true;
-    spmv_stream<T, kStreamK><<<grid, kBlock, 0, ctx->stream>>>(A->n_blk, A->d_blk, A->d_rp,
+    spmv_stream<T, kStreamK><<<grid, kBlock, 0, ctx->stream>>>(A->n_blk, A->d_meta, A->d_rp,
                                                               A->d_ci, v, x, y, ep);
     ctx->launches++;
     MTLGPU_TRY_CUDA(ctx, cudaGetLastError());

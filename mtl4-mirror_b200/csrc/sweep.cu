@@ -10,7 +10,8 @@
 // One launch per sweep.  The factor is stored in level order (SweepPlan);
 // warps claim tasks (<= 32/G rows of one level) through an atomic ticket in
 // level order, G lanes per row load the row's off-diagonal entries and wait
-// for each dependency w[j] to become final.  w is NaN-boxed (see device.cuh):
+// for each dependency w[j] to become final; the row's products are folded in
+// the reference's order (see sweep_kernel).  w is NaN-boxed (see device.cuh):
 // the output buffer is prefilled with the sentinel and a row's result is
 // published by a single relaxed store, so a dependency costs one L2 round
 // trip and no fence.  Every wait is bounded; on exhaustion the kernel records
@@ -31,6 +32,19 @@ namespace {
 
 constexpr int kBlock = 256;
 
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+// G lanes per row.  Lane gl of a row's group waits for w[c] of entries
+// gl, gl + G, ... and forms the separately rounded product a * w[c]; the
+// group's G products of one pass go to shared memory, and lane 0 folds them
+// into rr = v[r] in stored column order with separately rounded
+// subtractions, then w[r] = rr * dia: the reference's `rr -= value *
+// w[col]` loop, bit for bit.  (Folding through shared memory measured
+// 3x faster on B200 than a chain of width-G shuffles for FP64, and as fast as
+// the unordered shuffle tree it replaces.)
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock)
     sweep_kernel(int n_tasks, const int32_t* __restrict__ task_ptr, const int32_t* __restrict__ rp,
@@ -39,8 +53,10 @@ __global__ void __launch_bounds__(kBlock)
                  const T* __restrict__ in, T* out, unsigned* ticket, int* err, long long limit,
                  const int* skip, unsigned total_warps) {
   if (skip && ld_relaxed(skip)) return;
+  __shared__ T stage[kBlock];
   const int lane = threadIdx.x & 31;
   const int sub = lane / G, gl = lane % G;
+  T* st = stage + (threadIdx.x & ~31) + sub * G;
   while (true) {
     unsigned t = 0;
     if (lane == 0) t = atomicAdd(ticket, 1u);
@@ -48,24 +64,40 @@ __global__ void __launch_bounds__(kBlock)
     if (t >= (unsigned)n_tasks) break;
     const int p = task_ptr[t] + sub;
     const bool valid = p < task_ptr[t + 1];
-    T acc = T(0), rhs = T(0), d = T(1);
-    int row = 0;
+    T rr = T(0), d = T(1);
+    int row = 0, b = 0, len = 0;
     if (valid) {
       row = row_of[p];
-      rhs = in[row];
+      rr = in[row];
       if (dinv) d = dinv[p];
-      const int b = rp[p], e = rp[p + 1];
-      for (int j = b + gl; j < e; j += G) {
-        const int c = ci[j];
-        const T a = val[j];
-        acc += a * wait_value(out + c, limit, err);
+      b = rp[p];
+      len = rp[p + 1] - b;
+    }
+    if (G == 1) {
+      for (int j = 0; j < len; j++)
+        rr = sub_rn(rr, mul_rn(val[b + j], wait_value(out + ci[b + j], limit, err)));
+    } else {
+      // the same number of passes in every lane (the warp syncs per pass)
+      int passes = (len + G - 1) / G;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1)
+        passes = max(passes, __shfl_xor_sync(0xffffffffu, passes, off));
+      for (int ps = 0; ps < passes; ps++) {
+        const int k = ps * G + gl;
+        T prod = T(0);
+        if (k < len) prod = mul_rn(val[b + k], wait_value(out + ci[b + k], limit, err));
+        st[gl] = prod;
+        __syncwarp();
+        if (gl == 0) {
+          const int cnt = min(len - ps * G, G);
+          for (int q = 0; q < cnt; q++) rr = sub_rn(rr, st[q]);
+        }
+        __syncwarp();
       }
     }
-#pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if (valid && gl == 0) {
-      T res = rhs - acc;
-      if (dinv) res = res * d;
+      T res = rr;
+      if (dinv) res = mul_rn(res, d);
       st_relaxed(out + row, canonical(res));
     }
   }

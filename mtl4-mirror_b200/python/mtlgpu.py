@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "lib", "libmtlgpu.so")
+FIX_PATH = os.path.join(PKG, "lib", "libmtlgpu_fixtures.so")
 
 OK, MAX_ITER, INVALID_ARG, NOT_SQUARE, MISSING_DIAGONAL, ZERO_PIVOT, BREAKDOWN, TIMEOUT, \
     INTERRUPTED, CUDA_ERROR, NOT_SORTED, INDEX_RANGE, OUT_OF_MEMORY, INCOMPATIBLE_SIZE, \
@@ -67,17 +68,6 @@ def _lib():
         L.mtlgpu_status_string.restype = C.c_char_p
         L.mtlgpu_last_error.restype = C.c_char_p
         L.mtlgpu_ctx_stream.restype = _vp
-        for name in ("mtlgpu_gen_laplacian2d", "mtlgpu_gen_laplacian3d", "mtlgpu_gen_convdiff27",
-                     "mtlgpu_gen_random_graph", "mtlgpu_gen_fv2d", "mtlgpu_gen_graph_batch"):
-            getattr(L, name).restype = C.c_longlong
-        L.mtlgpu_gen_convdiff27.argtypes = [C.c_int, C.c_uint64, _vp, _vp, _vp]
-        L.mtlgpu_gen_random_graph.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, _vp,
-                                              _vp, _vp]
-        L.mtlgpu_gen_fv2d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, _vp, _vp, _vp]
-        L.mtlgpu_gen_graph_batch.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                             C.c_double, C.c_uint64, _vp, _vp, _vp, _vp]
-        L.mtlgpu_gen_uniform.argtypes = [C.c_longlong, C.c_uint64, C.c_double, C.c_double, _vp]
-        L.mtlgpu_gen_normal.argtypes = [C.c_longlong, C.c_uint64, _vp]
         L.mtlgpu_ctx_set_spin_limit.argtypes = [_vp, C.c_longlong]
         L.mtlgpu_malloc.argtypes = [_vp, C.c_size_t, C.POINTER(_vp)]
         L.mtlgpu_free.argtypes = [_vp, _vp]
@@ -91,6 +81,33 @@ def _lib():
         L.mtlgpu_unary_dot.argtypes = [_vp, C.c_int, _vp, C.POINTER(C.c_double)]
         _LIB = L
     return _LIB
+
+
+_FIX = None
+
+
+def _fix():
+    """libmtlgpu_fixtures: the seeded generators alone (include/mtlgpu_fixtures.h,
+    no CUDA), so that building inputs never maps the solver library."""
+    global _FIX
+    if _FIX is None:
+        if not os.path.exists(FIX_PATH):
+            raise OSError(f"libmtlgpu_fixtures not built: {FIX_PATH} missing "
+                          "(make -C mtl4-mirror_b200)")
+        L = C.CDLL(FIX_PATH)
+        for name in ("mtlgpu_gen_laplacian2d", "mtlgpu_gen_laplacian3d", "mtlgpu_gen_convdiff27",
+                     "mtlgpu_gen_random_graph", "mtlgpu_gen_fv2d", "mtlgpu_gen_graph_batch"):
+            getattr(L, name).restype = C.c_longlong
+        L.mtlgpu_gen_convdiff27.argtypes = [C.c_int, C.c_uint64, _vp, _vp, _vp]
+        L.mtlgpu_gen_random_graph.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, _vp,
+                                              _vp, _vp]
+        L.mtlgpu_gen_fv2d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, _vp, _vp, _vp]
+        L.mtlgpu_gen_graph_batch.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                             C.c_double, C.c_uint64, _vp, _vp, _vp, _vp]
+        L.mtlgpu_gen_uniform.argtypes = [C.c_longlong, C.c_uint64, C.c_double, C.c_double, _vp]
+        L.mtlgpu_gen_normal.argtypes = [C.c_longlong, C.c_uint64, _vp]
+        _FIX = L
+    return _FIX
 
 
 def lib():
@@ -243,6 +260,9 @@ class Csr:
     def spmv(self, x, y, alpha=1.0, beta=0.0):
         check(_lib().mtlgpu_spmv(self.h, x.ptr, y.ptr, float(alpha), float(beta)), "spmv")
 
+    def spmv_f32(self, x, y):
+        check(_lib().mtlgpu_spmv_f32(self.h, x.ptr, y.ptr), "spmv_f32")
+
     def spmv_transposed(self, x, y):
         check(_lib().mtlgpu_spmv_transposed(self.h, x.ptr, y.ptr), "spmv_transposed")
 
@@ -280,6 +300,10 @@ class Pc:
     def apply(self, r, z):
         check(_lib().mtlgpu_pc_apply(self.h, r.ptr, z.ptr), "pc_apply")
 
+    def apply_f32(self, r, z):
+        """FP32 apply (asynchronous; errors surface at ctx.synchronize())."""
+        check(_lib().mtlgpu_pc_apply_f32(self.h, r.ptr, z.ptr), "pc_apply_f32")
+
     def adjoint_apply(self, r, z):
         check(_lib().mtlgpu_pc_adjoint_apply(self.h, r.ptr, z.ptr), "pc_adjoint_apply")
 
@@ -288,6 +312,17 @@ class Pc:
             check(_lib().mtlgpu_pc_sweep_f32(self.h, which, x.ptr, y.ptr), "pc_sweep_f32")
         else:
             check(_lib().mtlgpu_pc_sweep(self.h, which, x.ptr, y.ptr), "pc_sweep")
+
+    def set_jacobi_sweeps(self, iters):
+        """Apply the triangular factors with `iters` Jacobi iterations per
+        triangle (0: the exact sweeps)."""
+        check(_lib().mtlgpu_pc_set_jacobi_sweeps(self.h, int(iters)), "pc_set_jacobi_sweeps")
+
+    def sweep_kind(self, which, prec=FP64):
+        """0: level-ordered sweep, 1: partitioned sweep, 2: Jacobi iterations."""
+        k = C.c_int()
+        check(_lib().mtlgpu_pc_sweep_kind(self.h, which, prec, C.byref(k)), "pc_sweep_kind")
+        return k.value
 
     def factor_info(self, which):
         nnz, lev = C.c_int(), C.c_int()
@@ -380,13 +415,8 @@ def solve_host_ptrs(method, A, P, x_ptr, b_ptr, **kw):
 
 # ---------------------------------------------------------------------------
 # fixtures (host generators)
-def _two_phase(fn, *args):
-    nnz = fn(*args, None, None, None)
-    return nnz
-
-
 def laplacian2d(m, n):
-    L = _lib()
+    L = _fix()
     nnz = L.mtlgpu_gen_laplacian2d(m, n, None, None, None)
     rp, ci, v = np.zeros(m * n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
     L.mtlgpu_gen_laplacian2d(m, n, _p(rp), _p(ci), _p(v))
@@ -394,7 +424,7 @@ def laplacian2d(m, n):
 
 
 def laplacian3d(N):
-    L = _lib()
+    L = _fix()
     nnz = L.mtlgpu_gen_laplacian3d(N, None, None, None)
     rp, ci, v = np.zeros(N ** 3 + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
     L.mtlgpu_gen_laplacian3d(N, _p(rp), _p(ci), _p(v))
@@ -402,7 +432,7 @@ def laplacian3d(N):
 
 
 def convdiff27(N, seed=2):
-    L = _lib()
+    L = _fix()
     nnz = L.mtlgpu_gen_convdiff27(N, seed, None, None, None)
     rp, ci, v = np.zeros(N ** 3 + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
     L.mtlgpu_gen_convdiff27(N, seed, _p(rp), _p(ci), _p(v))
@@ -410,7 +440,7 @@ def convdiff27(N, seed=2):
 
 
 def random_graph(n, avg_deg, shift_frac=1e-2, seed=3):
-    L = _lib()
+    L = _fix()
     nnz = L.mtlgpu_gen_random_graph(n, avg_deg, shift_frac, seed, None, None, None)
     rp, ci, v = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
     L.mtlgpu_gen_random_graph(n, avg_deg, shift_frac, seed, _p(rp), _p(ci), _p(v))
@@ -422,7 +452,7 @@ def graph_batch(count, n_min=1000, n_max=65536, deg_min=8.0, deg_max=32.0, shift
     """`count` random-graph Laplacians of log-uniform sizes (the batched-PCG
     workload): returns (systems, blockdiag) with systems a list of
     (n, rp, ci, v) and blockdiag = (n_total, rp, ci, v, offsets)."""
-    L = _lib()
+    L = _fix()
     sizes = np.zeros(2 * count, np.int64)
     total = L.mtlgpu_gen_graph_batch(count, n_min, n_max, deg_min, deg_max, shift_frac, seed,
                                      _p(sizes), None, None, None)
@@ -448,7 +478,7 @@ def graph_batch(count, n_min=1000, n_max=65536, deg_min=8.0, deg_max=32.0, shift
 
 
 def fv2d(N, sigma=1.0, corr=8.0, seed=4):
-    L = _lib()
+    L = _fix()
     nnz = L.mtlgpu_gen_fv2d(N, sigma, corr, seed, None, None, None)
     rp, ci, v = np.zeros(N * N + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
     L.mtlgpu_gen_fv2d(N, sigma, corr, seed, _p(rp), _p(ci), _p(v))
@@ -457,13 +487,13 @@ def fv2d(N, sigma=1.0, corr=8.0, seed=4):
 
 def uniform(n, seed, a=-1.0, b=1.0):
     out = np.zeros(n)
-    _lib().mtlgpu_gen_uniform(n, seed, a, b, _p(out))
+    _fix().mtlgpu_gen_uniform(n, seed, a, b, _p(out))
     return out
 
 
 def normal(n, seed):
     out = np.zeros(n)
-    _lib().mtlgpu_gen_normal(n, seed, _p(out))
+    _fix().mtlgpu_gen_normal(n, seed, _p(out))
     return out
 
 
@@ -471,5 +501,5 @@ def csr_mult(A, x):
     n, rp, ci, v = A
     x = np.ascontiguousarray(x, np.float64)
     y = np.zeros(n)
-    _lib().mtlgpu_gen_csr_mult(n, _p(rp), _p(ci), _p(v), _p(x), _p(y))
+    _fix().mtlgpu_gen_csr_mult(n, _p(rp), _p(ci), _p(v), _p(x), _p(y))
     return y

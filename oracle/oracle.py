@@ -198,9 +198,17 @@ class Restatement(_Base):
 class Reference(_Base):
     prefix = "ref_"
 
-    def __init__(self, path=None, openmp=False):
-        name = "libmtlref_omp.so" if openmp else "libmtlref.so"
-        super().__init__(path or os.path.join(HERE, "_ref", name))
+    FLAVOURS = {"parity": "libmtlref.so", "omp": "libmtlref_omp.so",
+                "serial": "libmtlref_serial.so"}
+
+    def __init__(self, path=None, openmp=False, flavour=None):
+        """flavour: 'parity' (-O2, no FMA contraction: the bit-comparable
+        oracle), 'omp' (-O3 -march=x86-64-v3 with OpenMP: the timed CPU
+        baseline on all cores), 'serial' (the same without OpenMP, CG's fused
+        loops active).  openmp=True is flavour 'omp'."""
+        flavour = flavour or ("omp" if openmp else "parity")
+        self.flavour = flavour
+        super().__init__(path or os.path.join(HERE, "_ref", self.FLAVOURS[flavour]))
         L = self.lib
         L.ref_spmv_time.restype = C.c_double
         L.ref_build_info.restype = C.c_char_p
@@ -246,10 +254,10 @@ class Reference(_Base):
         return (n, Lrp, Lci[:nl], Lv[:nl]), (n, Urp, Uci[:nu], Uv[:nu])
 
 
-def available_reference(openmp=False):
+def available_reference(openmp=False, flavour=None):
     """Reference() if its library was built (it is compiled where the
     reference tree exists and shipped prebuilt elsewhere), else None."""
     try:
-        return Reference(openmp=openmp)
+        return Reference(openmp=openmp, flavour=flavour)
     except (FileNotFoundError, OSError):
         return None

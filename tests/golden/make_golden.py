@@ -5,6 +5,7 @@ Run in a checkout where the reference tree is present (it is compiled by
 
     python tests/golden/make_golden.py            # small cases (seconds)
     python tests/golden/make_golden.py --cfg2     # + the 128^3 solve (about a minute)
+    python tests/golden/make_golden.py --cfg3     # + the 96^3 27-point BiCGSTAB solve
 
 Every array stored here is an output of the reference's own code path
 (laplacian_setup, compressed2D SpMV, ic_0 / ilu_0 factors, solve(P, x),
@@ -36,6 +37,7 @@ def put_csr(out, key, A):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
+    ap.add_argument("--cfg3", action="store_true")
     args = ap.parse_args()
     R = O.Reference()
     S = O.Restatement()
@@ -123,13 +125,22 @@ def main():
         rr = R.solve("cg", "ic0", A, b, rtol=1e-10, max_iter=2000)
         out["cfg2_iters"] = np.array([rr["iterations"], rr["err"]])
         out["cfg2_hist"] = rr["history"]
-    else:
-        old = os.path.join(HERE, "golden.npz")
-        if os.path.exists(old):
-            prev = np.load(old)
-            for k in ("cfg2_iters", "cfg2_hist"):
-                if k in prev:
-                    out[k] = prev[k]
+    if args.cfg3:
+        # 27-point convection-diffusion 96^3 (seed 2), x_true ~ U[-1,1] seed 1,
+        # b = A x_true by the reference's SpMV; FP64 bicgstab + ilu_0 to 1e-10
+        A = M.convdiff27(96, 2)
+        xt = M.uniform(A[0], 1)
+        b = R.spmv(A, xt)
+        rr = R.solve("bicgstab", "ilu0", A, b, rtol=1e-10, max_iter=2000)
+        out["cfg3_iters"] = np.array([rr["iterations"], rr["err"]])
+        out["cfg3_hist"] = rr["history"]
+        out["cfg3_b_sum"] = np.array([b.sum(), np.linalg.norm(b)])
+    old = os.path.join(HERE, "golden.npz")
+    if os.path.exists(old):
+        prev = np.load(old)
+        for k in prev.files:
+            if k.startswith(("cfg2_", "cfg3_")) and k not in out:
+                out[k] = prev[k]
 
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
     print("wrote", len(out), "arrays")

@@ -1,10 +1,10 @@
 """GPU kernels against the oracle, through the C ABI.
 
-Tolerances (stated per test): SpMV normwise relative error <= 1e-14 (FP64);
-factor values bit-identical (the device follows the reference's operation
-order with separate roundings); level arrays bit-exact; one triangular
-sweep / preconditioner apply <= 1e-12 relative (the device sums each row's
-products in a tree, the reference sequentially)."""
+Tolerances (stated per test): SpMV normwise relative error <= 1e-14 (FP64),
+and bit-identical where every row is summed in the reference's order;
+factor values, triangular sweeps and preconditioner applies bit-identical
+(the device follows the reference's operation order with separate
+roundings); level arrays bit-exact."""
 import numpy as np
 import pytest
 
@@ -88,28 +88,34 @@ def test_spmv_binned_rows(M, ctx, restate):
 
 
 def test_spmv_config_sizes(M, ctx, restate):
-    # full-size configurations: 128^3 7-point and 96^3 27-point
+    # full-size configurations: 128^3 7-point and 96^3 27-point; every row is
+    # summed in the reference's order, so the products are bit-identical
     for A in (M.laplacian3d(128), M.convdiff27(96, 2)):
         n = A[0]
         dA = M.Csr(ctx, *A[1:])
         x = M.uniform(n, 13)
         dx, dy = ctx.to_device(x), ctx.array(n)
         dA.spmv(dx, dy)
-        assert rel_err(dy.download(), restate.spmv(A, x)) <= 1e-14
+        ref = restate.spmv(A, x)
+        got = dy.download()
+        assert rel_err(got, ref) <= 1e-14
+        assert np.array_equal(got, ref)
         dA.close()
 
 
-def test_spmv_transposed(M, ctx):
-    A = M.convdiff27(6, 2)
-    n, rp, ci, v = A
-    rows = np.repeat(np.arange(n), np.diff(rp))
-    D = np.zeros((n, n))
-    D[rows, ci] = v
+@pytest.mark.parametrize("A_fn", [lambda M: M.convdiff27(6, 2), lambda M: M.convdiff27(20, 2),
+                                  lambda M: M.random_graph(1500, 12.0, 1e-2, 5)])
+def test_spmv_transposed(M, ctx, restate, A_fn):
+    # trans(A) * x (transposed_sparse_matrix_vector_product_test.cpp:32)
+    # against the oracle's SpMV with the oracle's CSR transpose
+    A = A_fn(M)
+    n = A[0]
     x = M.uniform(n, 9)
-    dA = M.Csr(ctx, rp, ci, v)
+    dA = M.Csr(ctx, *A[1:])
     dx, dy = ctx.to_device(x), ctx.array(n)
     dA.spmv_transposed(dx, dy)
-    assert rel_err(dy.download(), D.T @ x) <= 1e-14
+    ref = restate.spmv(restate.transpose(A), x)
+    assert rel_err(dy.download(), ref) <= 1e-14
 
 
 def test_csr_validation(M, ctx):
@@ -206,9 +212,13 @@ def test_pc_apply(M, ctx, restate, name, kind):
     r = M.uniform(n, 31)
     dr, dz = ctx.to_device(r), ctx.array(n)
     P.apply(dr, dz)
-    assert rel_err(dz.download(), restate.pc_apply(kind, A, r)) <= 1e-12
+    ref = restate.pc_apply(kind, A, r)
+    assert rel_err(dz.download(), ref) <= 1e-12
+    assert np.array_equal(dz.download(), ref)
     P.adjoint_apply(dr, dz)
-    assert rel_err(dz.download(), restate.pc_apply(kind, A, r, adjoint=True)) <= 1e-12
+    ref = restate.pc_apply(kind, A, r, adjoint=True)
+    assert rel_err(dz.download(), ref) <= 1e-12
+    assert np.array_equal(dz.download(), ref)
     # a second apply reuses the plans and must give the same bits
     z1 = dz.download()
     P.adjoint_apply(dr, dz)
@@ -220,34 +230,62 @@ def test_pc_apply_golden(M, ctx, golden):
     P = M.Pc(M.Csr(ctx, *A[1:]), "ic0")
     db, dz = ctx.to_device(golden["lap16_b"]), ctx.array(A[0])
     P.apply(db, dz)
-    assert rel_err(dz.download(), golden["lap16_pc_ic0_apply"]) <= 1e-12
+    assert np.array_equal(dz.download(), golden["lap16_pc_ic0_apply"])
     C = M.convdiff27(8, 2)
     P = M.Pc(M.Csr(ctx, *C[1:]), "ilu0")
     db, dz = ctx.to_device(golden["cd8_b"]), ctx.array(C[0])
     P.apply(db, dz)
-    assert rel_err(dz.download(), golden["cd8_pc_ilu0_apply"]) <= 1e-12
+    assert np.array_equal(dz.download(), golden["cd8_pc_ilu0_apply"])
     P.adjoint_apply(db, dz)
-    assert rel_err(dz.download(), golden["cd8_pc_ilu0_adjoint"]) <= 1e-12
+    assert np.array_equal(dz.download(), golden["cd8_pc_ilu0_adjoint"])
 
 
-def test_single_sweeps(M, ctx, restate):
-    A = M.laplacian3d(12)
+@pytest.mark.parametrize("A_fn", [lambda M: M.laplacian3d(12), lambda M: M.fv2d(40),
+                                  lambda M: M.random_graph(2500, 24.0, 1e-2, 6)])
+def test_single_sweeps(M, ctx, restate, A_fn):
+    # one triangular sweep, bit-identical with the reference's loops (the
+    # random graph has rows long enough for several passes of a lane group)
+    A = A_fn(M)
     n = A[0]
     P = M.Pc(M.Csr(ctx, *A[1:]), "ic0")
     L, U = restate.ic0(A)
     r = M.uniform(n, 41)
     dr, dy = ctx.to_device(r), ctx.array(n)
     P.sweep(M.LOWER, dr, dy)
-    assert rel_err(dy.download(), restate.sweep("lower_invdiag_last", L, r)) <= 1e-12
+    assert np.array_equal(dy.download(), restate.sweep("lower_invdiag_last", L, r))
     P.sweep(M.UPPER, dr, dy)
-    assert rel_err(dy.download(), restate.sweep("upper_invdiag_first", U, r)) <= 1e-12
+    assert np.array_equal(dy.download(), restate.sweep("upper_invdiag_first", U, r))
     C = M.convdiff27(6, 2)
     Q = M.Pc(M.Csr(ctx, *C[1:]), "ilu0")
     L, U = restate.ilu0(C)
     r = M.uniform(C[0], 42)
     dr, dy = ctx.to_device(r), ctx.array(C[0])
     Q.sweep(M.LOWER, dr, dy)
-    assert rel_err(dy.download(), restate.sweep("lower_unit", L, r)) <= 1e-12
+    assert np.array_equal(dy.download(), restate.sweep("lower_unit", L, r))
+    Q.sweep(M.UPPER, dr, dy)
+    assert np.array_equal(dy.download(), restate.sweep("upper_invdiag_first", U, r))
+
+
+def test_single_sweeps_fp32(M, ctx, restate):
+    # the FP32 sweep of the mixed solves: float factors, float vectors,
+    # separately rounded float products and differences in the reference's
+    # order (the restatement run in float arithmetic, through numpy)
+    A = M.laplacian3d(10)
+    n = A[0]
+    P = M.Pc(M.Csr(ctx, *A[1:]), "ic0", M.FP32)
+    L, _ = restate.ic0(A, as_float=True)
+    _, rp, ci, v = L
+    v32 = v.astype(np.float32)
+    r = M.uniform(n, 43).astype(np.float32)
+    ref = np.zeros(n, np.float32)
+    for i in range(n):
+        rr = r[i]
+        for j in range(rp[i], rp[i + 1] - 1):
+            rr = np.float32(rr - np.float32(v32[j] * ref[ci[j]]))
+        ref[i] = np.float32(rr * v32[rp[i + 1] - 1])
+    dr, dy = ctx.to_device(r), ctx.array(n, np.float32)
+    P.sweep(M.LOWER, dr, dy)
+    assert np.array_equal(dy.download(), ref)
 
 
 def test_missing_diagonal(M, ctx):

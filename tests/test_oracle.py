@@ -226,3 +226,12 @@ def test_ic0_as_written_differs_from_textbook(M, restate):
     inv = np.diag(Ud)
     # every off-diagonal entry is the original a_ki times the row's inverse diagonal
     assert np.allclose(offd, np.triu(A, 1) * inv[:, None], rtol=0, atol=0)
+
+
+def test_fixture_spmv_matches_reference_spmv(M, reference):
+    # b = A x_true: the GPU arm of the benchmark forms it with the generator
+    # library's CSR product, the reference arm with the reference's own SpMV;
+    # both sum each row in column order, so the right-hand sides are identical
+    for A in (M.laplacian3d(24), M.convdiff27(12, 2)):
+        x = M.uniform(A[0], 1)
+        assert np.array_equal(M.csr_mult(A, x), reference.spmv(A, x))
