@@ -226,6 +226,8 @@ mtlgpu_status mtlgpu_unary_dot(mtlgpu_ctx* ctx, int n, const double* d_x, double
  * more (never on a B200) returns MTLGPU_INCOMPATIBLE_SIZE.
  * The first call on a device looks up that device's copy of the array (set-up
  * done once per device); make that first call before any stream capture.
+ * Later calls check the address again, so the entry point stays valid after
+ * a cudaDeviceReset.
  * All calls on a device share the array, so calls whose kernels overlap on
  * the GPU race and give wrong results: order them (one stream, or events). */
 mtlgpu_status mtlgpu_dot_noalloc(int n, const double* d_x, const double* d_y, double* d_result,

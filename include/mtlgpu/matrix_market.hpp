@@ -58,14 +58,15 @@ inline csr_matrix read_matrix_market(std::istream& in) {
   std::string marker, object, format, field, symmetry;
   head >> marker >> object >> format >> field >> symmetry;
   if (marker != "%%MatrixMarket") throw format_error("File not in Matrix Market format");
-  if (lower(object) != "matrix") throw format_error("Try to read matrix from non-matrix file");
+  // object and field are compared as written, format and symmetry after
+  // lowering them (matrix_market.hpp:171-196)
+  if (object != "matrix") throw format_error("Try to read matrix from non-matrix file");
   format = lower(format);
-  field = lower(field);
   symmetry = lower(symmetry);
   if (format != "coordinate" && format != "array") throw format_error("unknown Matrix Market format");
   if (field == "complex") throw format_error("Cannot convert complex value in real");
-  if (field != "real" && field != "integer" && field != "pattern" && field != "double")
-    throw format_error("unknown Matrix Market field");
+  if (field != "real" && field != "integer" && field != "pattern")
+    throw format_error("Unknown tag for matrix value type in file");
   int sym = 0;  // 0 general, 1 symmetric/hermitian, -1 skew
   if (symmetry == "symmetric" || symmetry == "hermitian")
     sym = 1;
@@ -96,8 +97,13 @@ inline csr_matrix read_matrix_market(std::istream& in) {
       long long i, j;
       double v = 0;
       if (!(in >> i >> j)) break;  // fewer entries than announced: stop, as the reference does
-      if (field != "pattern" && !(in >> v)) throw format_error("missing value");
-      if (field == "pattern") v = 0.0;
+      if (field == "integer") {    // read as an integer, as the reference reads a long
+        long long iv = 0;
+        if (!(in >> iv)) throw format_error("missing value");
+        v = (double)iv;
+      } else if (field == "real") {
+        if (!(in >> v)) throw format_error("missing value");
+      }
       put(i - 1, j - 1, v);
       if (i != j && sym != 0) put(j - 1, i - 1, sym * v);
     }
@@ -105,7 +111,13 @@ inline csr_matrix read_matrix_market(std::istream& in) {
     for (long long c = 0; c < cols; ++c)
       for (long long r = 0; r < rows; ++r) {
         double v = 0;
-        if (!(in >> v)) throw format_error("missing array value");
+        if (field == "integer") {
+          long long iv = 0;
+          if (!(in >> iv)) throw format_error("missing array value");
+          v = (double)iv;
+        } else if (field != "pattern" && !(in >> v)) {
+          throw format_error("missing array value");
+        }
         put(r, c, v);
       }
   }

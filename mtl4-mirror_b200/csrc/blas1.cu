@@ -115,6 +115,8 @@ mtlgpu_status axpby_launch(Ctx* ctx, int n, double alpha, const double* x, doubl
 // without ordering) race on it and give wrong results.  The first call on each
 // device does that device's set-up (cudaGetSymbolAddress of the array, with the
 // device current); that first call should come before any stream capture.
+// Later calls look the address up again, so a call after cudaDeviceReset
+// (which reloads the module) uses the array's current address.
 namespace {
 constexpr int kNoAllocPartials = 4096;
 constexpr size_t kNoAllocCounterOffset = kNoAllocPartials * sizeof(double);
@@ -139,7 +141,17 @@ mtlgpu_status noalloc_setup(int device, NoAllocDevice** out) {
   if (device < 0 || device >= kNoAllocMaxDevices) return MTLGPU_INVALID_ARG;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   NoAllocDevice& d = g_noalloc_dev[device];
-  if (!d.ready) {
+  if (d.ready) {
+    // A cudaDeviceReset reloads the module, which may place the array
+    // elsewhere: look the address up again (cheap after the first time) and
+    // keep the current one.
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_dot_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return MTLGPU_CUDA_ERROR;
+    }
+    d.scratch = static_cast<unsigned char*>(p);
+  } else {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_dot_noalloc_scratch) != cudaSuccess || !p) {
       cudaGetLastError();

@@ -242,6 +242,27 @@ __device__ __forceinline__ R reduce_partials(const R* partials, int count) {
   return block_reduce(acc);
 }
 
+// 16-byte vector access: VN<T> elements per load / store (4 floats, 2
+// doubles).  The pointer must be 16-byte aligned (every library buffer is).
+template <typename T>
+struct VN {
+  static constexpr int value = 16 / (int)sizeof(T);
+};
+__device__ __forceinline__ void ld16(const float* p, float (&o)[4]) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  o[0] = v.x, o[1] = v.y, o[2] = v.z, o[3] = v.w;
+}
+__device__ __forceinline__ void ld16(const double* p, double (&o)[2]) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  o[0] = v.x, o[1] = v.y;
+}
+__device__ __forceinline__ void st16(float* p, const float (&o)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void st16(double* p, const double (&o)[2]) {
+  *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+}
+
 // Grid-stride loop bounds helper.
 __device__ __forceinline__ long long gtid() {
   return (long long)blockIdx.x * blockDim.x + threadIdx.x;

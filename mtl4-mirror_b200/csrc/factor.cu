@@ -584,8 +584,8 @@ mtlgpu_status pc_set_jacobi(Pc* P, int iters) {
     const bool f32 = P->prec == MTLGPU_FP32;
     const int lower_diag = P->kind == MTLGPU_PC_IC0 ? 2 : 0;
     MTLGPU_TRY(sell_build(ctx, P->n, P->d_Lrp, P->d_Lci, P->d_Lv, lower_diag, true, f32, f32,
-                          &P->jac_lower));
-    MTLGPU_TRY(sell_build(ctx, P->n, P->d_Urp, P->d_Uci, P->d_Uv, 1, true, f32, f32,
+                          true, &P->jac_lower));
+    MTLGPU_TRY(sell_build(ctx, P->n, P->d_Urp, P->d_Uci, P->d_Uv, 1, true, f32, f32, true,
                           &P->jac_upper));
     MTLGPU_TRY(dalloc(ctx, &P->d_jtmp, P->n));
     if (f32) MTLGPU_TRY(dalloc(ctx, &P->d_jtmp32, P->n));

@@ -60,6 +60,7 @@ struct Sell {
   int max_width = 0;               // largest slice width (entries per row)
   bool unit_diag = false;
   bool round64 = false;            // double copy holds float-rounded values
+  bool col_scaled = false;         // entry (r, c) stored as a_rc * dinv[c]
   int32_t* d_slice_ptr = nullptr;  // n_slices + 1 entry offsets (multiples of 32)
   int32_t* d_col = nullptr;
   double* d_val = nullptr;
@@ -247,7 +248,7 @@ mtlgpu_status part_sweep_launch(Ctx* ctx, const SweepPlan& S, const T* in, T* ou
 long long sell_padded_entries(int n, const int32_t* h_rp, int diag_pos);
 mtlgpu_status sell_build(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_ci,
                          const double* d_v, int diag_pos, bool fp64, bool fp32, bool round64,
-                         Sell* J);
+                         bool scale_cols, Sell* J);
 mtlgpu_status sell_refill(Ctx* ctx, const int32_t* d_rp, const int32_t* d_ci, const double* d_v,
                           int diag_pos, Sell* J);
 mtlgpu_status sell_ensure_fp32(Ctx* ctx, const int32_t* d_rp, const int32_t* d_ci,

@@ -52,19 +52,21 @@ struct PassDot {
   unsigned* counter = nullptr;
 };
 
-// One Jacobi iteration of one triangle.  FIRST: the previous iterate is
-// w_0 = D v, formed on the fly from v (and D) at the gathered columns.  The
-// entries of a row are taken in chunks of C: all C column indices and values
-// are loaded, then all C gathers issued, so a row costs one DRAM and one L2
-// round trip per chunk rather than per entry.
-// 8 resident CTAs (32 registers) for the FP32 chunk-4 form the 7-point
-// factors of the mixed solves use; 6 where more state per thread would spill.
-template <typename T, bool FIRST, bool UNIT, bool DOT, int C>
+// One Jacobi iteration of one triangle in the scaled form.  With the
+// off-diagonal part stored column-scaled, Nt = N D (sell.cu), the iteration
+// w_{m+1} = D (v - N w_m), w_0 = D v, is w_m = D u_m with
+//     u_0 = v,   u_{m+1} = v - Nt u_m,
+// so every pass gathers one vector and only the last one (SCALE) multiplies
+// by D.  For ILU(0)'s unit lower factor D = I and Nt = N.  The entries of a
+// row are taken in chunks of C: all C column indices and values are loaded
+// (last-use hint), then all C gathers issued, so a row costs one DRAM and
+// one L2 round trip per chunk.
+template <typename T, bool SCALE, bool DOT, int C>
 __global__ void __launch_bounds__(kBlock, (C == 4 && sizeof(T) == 4) ? 8 : 6)
     jacobi_pass_kernel(int n, const int32_t* __restrict__ slice_ptr,
                        const int32_t* __restrict__ col, const T* __restrict__ val,
                        const T* __restrict__ dinv, const T* __restrict__ v,
-                       const T* __restrict__ w_in, T* __restrict__ w_out, const int* skip,
+                       const T* __restrict__ in, T* __restrict__ out, const int* skip,
                        PassDot dot) {
   if (skip && ld_relaxed(skip)) return;
   typedef typename AccOf<T, 1>::type R;
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(kBlock, (C == 4 && sizeof(T) == 4) ? 8 : 6)
     const int base = __ldg(slice_ptr + s);
     const int width = (__ldg(slice_ptr + s + 1) - base) >> 5;
     const T vr = __ldg(v + r);
-    const T dr = UNIT ? T(1) : __ldg(dinv + r);
+    const T dr = SCALE ? __ldg(dinv + r) : T(1);
     const int32_t* cp = col + base + lane;
     const T* vp = val + base + lane;
     T acc = T(0);
@@ -84,26 +86,18 @@ __global__ void __launch_bounds__(kBlock, (C == 4 && sizeof(T) == 4) ? 8 : 6)
       T a[C], x[C];
 #pragma unroll
       for (int u = 0; u < C; u++) {
-        const bool in = k0 + u < width;
-        c[u] = in ? __ldlu(cp + 32 * (k0 + u)) : -1;
-        a[u] = in ? __ldlu(vp + 32 * (k0 + u)) : T(0);
+        const bool inr = k0 + u < width;
+        c[u] = inr ? __ldlu(cp + 32 * (k0 + u)) : -1;
+        a[u] = inr ? __ldlu(vp + 32 * (k0 + u)) : T(0);
       }
 #pragma unroll
-      for (int u = 0; u < C; u++) {
-        const bool in = c[u] >= 0;  // -1: padding
-        if (FIRST) {
-          x[u] = in ? __ldg(v + c[u]) : T(0);
-          if (!UNIT) x[u] *= in ? __ldg(dinv + c[u]) : T(0);
-        } else {
-          x[u] = in ? __ldg(w_in + c[u]) : T(0);
-        }
-      }
+      for (int u = 0; u < C; u++) x[u] = c[u] >= 0 ? __ldg(in + c[u]) : T(0);  // -1: padding
 #pragma unroll
       for (int u = 0; u < C; u++) acc += a[u] * x[u];
     }
     T res = vr - acc;
-    if (!UNIT) res *= dr;
-    w_out[r] = res;
+    if (SCALE) res *= dr;
+    out[r] = res;
     if (DOT) acc_dot.add_prod(0, __ldg(static_cast<const T*>(dot.with) + r), res);
   }
   if (DOT) {
@@ -130,13 +124,13 @@ struct JVals<float> {
 };
 
 // Chunk width C: 4 when no row has more than 4 off-diagonal entries (the
-// 7-point factors), else 8 (fewer registers for the short rows).
-template <typename T, bool FIRST, bool UNIT>
-void launch3(int grid, cudaStream_t st, const Sell& J, const T* val, const T* dinv,
-             const T* v, const T* w_in, T* w_out, const int* skip, const PassDot& dot) {
+// 7-point factors), else 8.
+template <typename T, bool SCALE>
+void launch2(int grid, cudaStream_t st, const Sell& J, const T* val, const T* dinv, const T* v,
+             const T* in, T* out, const int* skip, const PassDot& dot) {
 #define MTLGPU_JP(DOT, C)                                                               \
-  jacobi_pass_kernel<T, FIRST, UNIT, DOT, C><<<grid, kBlock, 0, st>>>(                  \
-      J.n, J.d_slice_ptr, J.d_col, val, dinv, v, w_in, w_out, skip, dot)
+  jacobi_pass_kernel<T, SCALE, DOT, C><<<grid, kBlock, 0, st>>>(                        \
+      J.n, J.d_slice_ptr, J.d_col, val, dinv, v, in, out, skip, dot)
   if (J.max_width <= 4) {
     if (dot.out) MTLGPU_JP(true, 4); else MTLGPU_JP(false, 4);
   } else {
@@ -146,24 +140,16 @@ void launch3(int grid, cudaStream_t st, const Sell& J, const T* val, const T* di
 }
 
 template <typename T>
-mtlgpu_status pass_launch(Ctx* ctx, const Sell& J, bool first, const T* v, const T* w_in,
-                          T* w_out, const int* skip, const PassDot& dot) {
+mtlgpu_status pass_launch(Ctx* ctx, const Sell& J, bool scale, const T* v, const T* in, T* out,
+                          const int* skip, const PassDot& dot) {
   const T* val = JVals<T>::val(J);
   const T* dinv = JVals<T>::dinv(J);
-  if (!val || (!J.unit_diag && !dinv)) return MTLGPU_INVALID_ARG;
+  if (!val || (scale && !dinv) || (!J.unit_diag && !J.col_scaled)) return MTLGPU_INVALID_ARG;
   const int grid = grid_rows(ctx, J.n);
-  cudaStream_t st = ctx->stream;
-  if (first) {
-    if (J.unit_diag)
-      launch3<T, true, true>(grid, st, J, val, dinv, v, w_in, w_out, skip, dot);
-    else
-      launch3<T, true, false>(grid, st, J, val, dinv, v, w_in, w_out, skip, dot);
-  } else {
-    if (J.unit_diag)
-      launch3<T, false, true>(grid, st, J, val, dinv, v, w_in, w_out, skip, dot);
-    else
-      launch3<T, false, false>(grid, st, J, val, dinv, v, w_in, w_out, skip, dot);
-  }
+  if (scale)
+    launch2<T, true>(grid, ctx->stream, J, val, dinv, v, in, out, skip, dot);
+  else
+    launch2<T, false>(grid, ctx->stream, J, val, dinv, v, in, out, skip, dot);
   ctx->launches++;
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
@@ -180,7 +166,7 @@ template <typename T>
 mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T* scratch,
                            const int* skip, const T* dot_with, double* dot_out) {
   if (J.n == 0) return MTLGPU_OK;
-  const T* prev = nullptr;
+  const T* prev = v;  // u_0 = v
   for (int i = 0; i < k; i++) {
     T* dst = ((k - 1 - i) % 2 == 0) ? out : scratch;
     PassDot dot;
@@ -190,7 +176,7 @@ mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T
       dot.partials = ctx->d_partials;
       dot.counter = counter_slot(ctx, 9);
     }
-    MTLGPU_TRY(pass_launch<T>(ctx, J, i == 0, v, prev, dst, skip, dot));
+    MTLGPU_TRY(pass_launch<T>(ctx, J, i == k - 1 && !J.unit_diag, v, prev, dst, skip, dot));
     prev = dst;
   }
   return MTLGPU_OK;

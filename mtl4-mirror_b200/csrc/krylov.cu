@@ -103,15 +103,29 @@ __global__ void init_check_kernel(SolverState* st, bool identity_pc) {
   if (iter_finished(st, sqrt(fabs(rr)))) st->done = 1;
 }
 
+// Vectorised element loops: thread i handles the 16-byte vector i (V
+// elements) of every array, grid-stride; the n mod V tail element-wise.
+#define MTLGPU_VLOOP(n, V)                                                         \
+  for (long long i0 = gtid() * (V); i0 + (V) <= (n); i0 += gstride() * (V))
+#define MTLGPU_TAIL(n, V) for (long long i = ((n) / (V)) * (V) + gtid(); i < (n); i += gstride())
+
 // rho = r . z
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     cg_rho_kernel(int n, const T* __restrict__ r, const T* __restrict__ z, SolverState* st,
                   void* partials, unsigned* counter) {
   if (st->done) return;
   typedef typename AccOf<T, 1>::type R;
+  constexpr int V = VN<T>::value;
   R acc = R::zero();
-  for (long long i = gtid(); i < n; i += gstride()) acc.add_prod(0, r[i], z[i]);
+  MTLGPU_VLOOP(n, V) {
+    T rv[V], zv[V];
+    ld16(r + i0, rv);
+    ld16(z + i0, zv);
+#pragma unroll
+    for (int u = 0; u < V; u++) acc.add_prod(0, rv[u], zv[u]);
+  }
+  MTLGPU_TAIL(n, V) acc.add_prod(0, r[i], z[i]);
   R bs = block_reduce(acc);
   R* parts = reinterpret_cast<R*>(partials);
   if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
@@ -122,30 +136,63 @@ __global__ void __launch_bounds__(kBlock)
 
 // p = z (first iteration) | z + (rho / rho_1) p   (cg.hpp:99-102, 57-60)
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     cg_p_kernel(int n, const T* __restrict__ z, T* __restrict__ p, const SolverState* st) {
   if (st->done) return;
+  constexpr int V = VN<T>::value;
   if (st->iter == 0) {
-    for (long long i = gtid(); i < n; i += gstride()) p[i] = z[i];
+    MTLGPU_VLOOP(n, V) {
+      T zv[V];
+      ld16(z + i0, zv);
+      st16(p + i0, zv);
+    }
+    MTLGPU_TAIL(n, V) p[i] = z[i];
     return;
   }
   const T beta = (T)(st->rho / st->rho_1);
-  for (long long i = gtid(); i < n; i += gstride()) p[i] = z[i] + beta * p[i];
+  MTLGPU_VLOOP(n, V) {
+    T zv[V], pv[V];
+    ld16(z + i0, zv);
+    ld16(p + i0, pv);
+#pragma unroll
+    for (int u = 0; u < V; u++) pv[u] = zv[u] + beta * pv[u];
+    st16(p + i0, pv);
+  }
+  MTLGPU_TAIL(n, V) p[i] = z[i] + beta * p[i];
 }
 
 // alpha = rho / alpha_1; x += alpha p; r -= alpha q; rr = r . r; next test.
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     cg_update_kernel(int n, T* __restrict__ x, const T* __restrict__ p, T* __restrict__ r,
                      const T* __restrict__ q, T* fill_a, T* fill_b, SolverState* st,
                      bool identity_pc, void* partials, unsigned* counter) {
   if (st->done) return;
   typedef typename AccOf<T, 1>::type R;
+  constexpr int V = VN<T>::value;
   const double alpha_d = st->rho / st->alpha_1;
   const T alpha = (T)alpha_d;
   const T s = Box<T>::sentinel();
   R acc = R::zero();
-  for (long long i = gtid(); i < n; i += gstride()) {
+  MTLGPU_VLOOP(n, V) {
+    T xv[V], pv[V], rv[V], qv[V], sv[V];
+    ld16(x + i0, xv);
+    ld16(p + i0, pv);
+    ld16(r + i0, rv);
+    ld16(q + i0, qv);
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+      xv[u] += alpha * pv[u];
+      rv[u] = rv[u] - alpha * qv[u];
+      acc.add_prod(0, rv[u], rv[u]);
+      sv[u] = s;
+    }
+    st16(x + i0, xv);
+    st16(r + i0, rv);
+    if (fill_a) st16(fill_a + i0, sv);
+    if (fill_b) st16(fill_b + i0, sv);
+  }
+  MTLGPU_TAIL(n, V) {
     x[i] += alpha * p[i];
     const T ri = r[i] - alpha * q[i];
     r[i] = ri;
@@ -171,13 +218,21 @@ __global__ void __launch_bounds__(kBlock)
 // ---- BiCGSTAB -------------------------------------------------------------
 // rho_1 = rtilde . r, breakdown tests (bicgstab.hpp:45-52), ++iter.
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     bicg_rho_kernel(int n, const T* __restrict__ rt, const T* __restrict__ r, SolverState* st,
                     void* partials, unsigned* counter) {
   if (st->done) return;
   typedef typename AccOf<T, 1>::type R;
+  constexpr int V = VN<T>::value;
   R acc = R::zero();
-  for (long long i = gtid(); i < n; i += gstride()) acc.add_prod(0, rt[i], r[i]);
+  MTLGPU_VLOOP(n, V) {
+    T a[V], c[V];
+    ld16(rt + i0, a);
+    ld16(r + i0, c);
+#pragma unroll
+    for (int u = 0; u < V; u++) acc.add_prod(0, a[u], c[u]);
+  }
+  MTLGPU_TAIL(n, V) acc.add_prod(0, rt[i], r[i]);
   R bs = block_reduce(acc);
   R* parts = reinterpret_cast<R*>(partials);
   if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
@@ -197,24 +252,39 @@ __global__ void __launch_bounds__(kBlock)
 
 // p = r (first) | r + beta (p - omega v), beta = (rho_1/rho_2)(alpha/omega)
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     bicg_p_kernel(int n, const T* __restrict__ r, T* __restrict__ p, const T* __restrict__ v,
                   const SolverState* st) {
   if (st->done) return;
+  constexpr int V = VN<T>::value;
   if (st->iter <= 1) {
-    for (long long i = gtid(); i < n; i += gstride()) p[i] = r[i];
+    MTLGPU_VLOOP(n, V) {
+      T a[V];
+      ld16(r + i0, a);
+      st16(p + i0, a);
+    }
+    MTLGPU_TAIL(n, V) p[i] = r[i];
     return;
   }
   // st->rho_1 holds rho_2 (previous rho), st->alpha_1 the previous alpha
   const double beta_d = (st->rho / st->rho_1) * (st->alpha_1 / st->omega);
   const T beta = (T)beta_d, omega = (T)st->omega;
-  for (long long i = gtid(); i < n; i += gstride()) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+  MTLGPU_VLOOP(n, V) {
+    T rv[V], pv[V], vv[V];
+    ld16(r + i0, rv);
+    ld16(p + i0, pv);
+    ld16(v + i0, vv);
+#pragma unroll
+    for (int u = 0; u < V; u++) pv[u] = rv[u] + beta * (pv[u] - omega * vv[u]);
+    st16(p + i0, pv);
+  }
+  MTLGPU_TAIL(n, V) p[i] = r[i] + beta * (p[i] - omega * v[i]);
 }
 
 // alpha = rho_1 / gamma; s = r - alpha v; ||s||; half-step termination test
 // (bicgstab.hpp:58-67).
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     bicg_s_kernel(int n, const T* __restrict__ r, const T* __restrict__ v, T* __restrict__ s,
                   T* fill_a, T* fill_b, SolverState* st, void* partials, unsigned* counter) {
   if (st->done) return;
@@ -222,8 +292,23 @@ __global__ void __launch_bounds__(kBlock)
   const double gamma = st->gamma;
   const T alpha = (T)(st->rho / gamma);
   const T sent = Box<T>::sentinel();
+  constexpr int V = VN<T>::value;
   R acc = R::zero();
-  for (long long i = gtid(); i < n; i += gstride()) {
+  MTLGPU_VLOOP(n, V) {
+    T rv[V], vv[V], sv[V], fv[V];
+    ld16(r + i0, rv);
+    ld16(v + i0, vv);
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+      sv[u] = rv[u] - alpha * vv[u];
+      acc.add_prod(0, sv[u], sv[u]);
+      fv[u] = sent;
+    }
+    st16(s + i0, sv);
+    if (fill_a) st16(fill_a + i0, fv);
+    if (fill_b) st16(fill_b + i0, fv);
+  }
+  MTLGPU_TAIL(n, V) {
     const T si = r[i] - alpha * v[i];
     s[i] = si;
     acc.add_prod(0, si, si);
@@ -254,15 +339,24 @@ __global__ void __launch_bounds__(kBlock)
 // x += omega shat + alpha phat, r = s - omega t, ||r|| and the loop test
 // (bicgstab.hpp:70-75, 43); on a half-step exit only x += alpha phat.
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     bicg_x_kernel(int n, T* __restrict__ x, const T* __restrict__ phat, const T* __restrict__ shat,
                   const T* __restrict__ s, const T* __restrict__ t, T* __restrict__ r, T* fill_a,
                   T* fill_b, SolverState* st, void* partials, unsigned* counter) {
   if (st->done) return;
   typedef typename AccOf<T, 1>::type R;
   const T alpha = (T)st->alpha_1;
+  constexpr int V = VN<T>::value;
   if (st->half_exit) {
-    for (long long i = gtid(); i < n; i += gstride()) x[i] += alpha * phat[i];
+    MTLGPU_VLOOP(n, V) {
+      T xv[V], ph[V];
+      ld16(x + i0, xv);
+      ld16(phat + i0, ph);
+#pragma unroll
+      for (int u = 0; u < V; u++) xv[u] += alpha * ph[u];
+      st16(x + i0, xv);
+    }
+    MTLGPU_TAIL(n, V) x[i] += alpha * phat[i];
     __syncthreads();
     if (publish_partial(R::zero(), reinterpret_cast<R*>(partials), blockIdx.x, counter,
                         gridDim.x)) {
@@ -274,7 +368,26 @@ __global__ void __launch_bounds__(kBlock)
   const T omega = (T)omega_d;
   const T sent = Box<T>::sentinel();
   R acc = R::zero();
-  for (long long i = gtid(); i < n; i += gstride()) {
+  MTLGPU_VLOOP(n, V) {
+    T xv[V], sh[V], ph[V], sv[V], tv[V], fv[V];
+    ld16(x + i0, xv);
+    ld16(shat + i0, sh);
+    ld16(phat + i0, ph);
+    ld16(s + i0, sv);
+    ld16(t + i0, tv);
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+      xv[u] += omega * sh[u] + alpha * ph[u];
+      sv[u] = sv[u] - omega * tv[u];  // r
+      acc.add_prod(0, sv[u], sv[u]);
+      fv[u] = sent;
+    }
+    st16(x + i0, xv);
+    st16(r + i0, sv);
+    if (fill_a) st16(fill_a + i0, fv);
+    if (fill_b) st16(fill_b + i0, fv);
+  }
+  MTLGPU_TAIL(n, V) {
     x[i] += omega * shat[i] + alpha * phat[i];
     const T ri = s[i] - omega * t[i];
     r[i] = ri;
@@ -298,13 +411,24 @@ __global__ void __launch_bounds__(kBlock)
 
 // t . s and t . t after t = A shat (omega = dot(t,s) / dot(t,t)).
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 4)
     bicg_omega_kernel(int n, const T* __restrict__ t, const T* __restrict__ s, SolverState* st,
                       void* partials, unsigned* counter) {
   if (st->done || st->skip2) return;
   typedef typename AccOf<T, 2>::type R;
+  constexpr int V = VN<T>::value;
   R acc = R::zero();
-  for (long long i = gtid(); i < n; i += gstride()) {
+  MTLGPU_VLOOP(n, V) {
+    T tv[V], sv[V];
+    ld16(t + i0, tv);
+    ld16(s + i0, sv);
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+      acc.add_prod(0, tv[u], sv[u]);
+      acc.add_prod(1, tv[u], tv[u]);
+    }
+  }
+  MTLGPU_TAIL(n, V) {
     acc.add_prod(0, t[i], s[i]);
     acc.add_prod(1, t[i], t[i]);
   }
@@ -619,11 +743,13 @@ mtlgpu_status run_iterations(Workspace<T>* W, const volatile int* h_interrupt, i
       *interrupted = 1;
       break;
     }
+    // the error word is read after the graph: a bounded wait that ran out
+    // inside it ends the solve at once
     int err = 0;
-    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
-                                         ctx->stream));
     MTLGPU_TRY_CUDA(ctx, cudaGraphLaunch(W->exec, ctx->stream));
     ctx->launches += (long long)W->graph_nodes;
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
     MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (err) break;
   }

@@ -61,13 +61,22 @@ __global__ void slice_width_kernel(int n, int n_slices, const int32_t* __restric
   }
 }
 
+// The stored diagonal of row r (diag_pos 1: first entry, 2: last entry).
+__device__ __forceinline__ double diag_of(const int32_t* rp, const double* v, int r,
+                                          int diag_pos) {
+  return v[diag_pos == 1 ? rp[r] : rp[r + 1] - 1];
+}
+
 // Scatter the off-diagonal entries into the slices; pad; copy the diagonal.
+// scale_cols: each entry (r, c) is stored multiplied by the stored diagonal
+// of row c (the factor N D of the Jacobi solves); with round64 both factors
+// are the float values, whose product a double holds exactly.
 __global__ void slice_fill_kernel(int n, const int32_t* __restrict__ rp,
                                   const int32_t* __restrict__ ci, const double* __restrict__ v,
                                   int diag_pos, const int32_t* __restrict__ slice_ptr,
                                   int32_t* __restrict__ col, double* __restrict__ val,
                                   float* __restrict__ val32, double* __restrict__ dinv,
-                                  float* __restrict__ dinv32, bool round64) {
+                                  float* __restrict__ dinv32, bool round64, bool scale_cols) {
   for (long long r = gtid(); r < n; r += gstride()) {
     const long long s = r >> 5;
     const int lane = (int)(r & 31);
@@ -79,14 +88,20 @@ __global__ void slice_fill_kernel(int n, const int32_t* __restrict__ rp,
       const long long o = base + 32ll * k + lane;
       const bool real = j < e;
       col[o] = real ? ci[j] : -1;
-      const double a = real ? v[j] : 0.0;
+      double a = real ? v[j] : 0.0;
       // round64: the double copy holds the float values (FP32 factors are
       // applied at their float values, as the exact sweeps do)
-      if (val) val[o] = round64 ? (double)(float)a : a;
+      if (round64) a = (double)(float)a;
+      if (scale_cols && real) {
+        double dc = diag_of(rp, v, ci[j], diag_pos);
+        if (round64) dc = (double)(float)dc;
+        a *= dc;
+      }
+      if (val) val[o] = a;
       if (val32) val32[o] = (float)a;
     }
     if (diag_pos) {
-      const double d = v[diag_pos == 1 ? rp[r] : rp[r + 1] - 1];
+      const double d = diag_of(rp, v, (int)r, diag_pos);
       if (dinv) dinv[r] = round64 ? (double)(float)d : d;
       if (dinv32) dinv32[r] = (float)d;
     }
@@ -112,12 +127,14 @@ long long sell_padded_entries(int n, const int32_t* h_rp, int diag_pos) {
 }
 
 // fp64 / fp32: which value copies to hold; round64: the double copy holds
-// the float-rounded values (FP32 factors).
+// the float-rounded values (FP32 factors); scale_cols: entries stored times
+// the stored diagonal of their column's row (needs diag_pos != 0).
 mtlgpu_status sell_build(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_ci,
                          const double* d_v, int diag_pos, bool fp64, bool fp32, bool round64,
-                         Sell* J) {
+                         bool scale_cols, Sell* J) {
   J->n = n;
   J->round64 = round64;
+  J->col_scaled = scale_cols && diag_pos != 0;
   J->unit_diag = diag_pos == 0;
   J->n_slices = (n + 31) / 32;
   if (n == 0) return MTLGPU_OK;
@@ -154,7 +171,7 @@ mtlgpu_status sell_build(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_
   }
   slice_fill_kernel<<<grid_rows(ctx, n), kBlock, 0, ctx->stream>>>(
       n, d_rp, d_ci, d_v, diag_pos, J->d_slice_ptr, J->d_col, J->d_val, J->d_val32, J->d_dinv,
-      J->d_dinv32, J->round64);
+      J->d_dinv32, J->round64, J->col_scaled);
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
 }
@@ -175,7 +192,7 @@ mtlgpu_status sell_refill(Ctx* ctx, const int32_t* d_rp, const int32_t* d_ci, co
   if (J->n == 0) return MTLGPU_OK;
   slice_fill_kernel<<<grid_rows(ctx, J->n), kBlock, 0, ctx->stream>>>(
       J->n, d_rp, d_ci, d_v, diag_pos, J->d_slice_ptr, J->d_col, J->d_val, J->d_val32, J->d_dinv,
-      J->d_dinv32, J->round64);
+      J->d_dinv32, J->round64, J->col_scaled);
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
 }

@@ -391,7 +391,7 @@ mtlgpu_status csr_analyse(Csr* A) {
     }
     if (A->spmv_kernel == 2)
       MTLGPU_TRY(sell_build(ctx, A->n_rows, A->d_rp, A->d_ci, A->d_v, 0, true, false, false,
-                            &A->sell));
+                            false, &A->sell));
     const int cap = 32 * kStreamK;
     std::vector<int2> blk;
     blk.reserve(A->n_rows / 16 + 2);

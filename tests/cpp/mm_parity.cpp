@@ -23,6 +23,19 @@ const char* kCases[][2] = {
     {"integer", "%%MatrixMarket matrix coordinate integer symmetric\n3 3 3\n1 1 5\n3 1 -2\n3 3 9\n"},
     {"duplicate", "%%MatrixMarket matrix coordinate real general\n2 2 3\n1 1 1\n1 1 3\n2 2 5\n"},
     {"array", "%%MatrixMarket matrix array real general\n2 3\n1\n2\n0\n4\n5\n6\n"},
+    // an integer file holding a fraction: the value is read as an integer
+    // and the reader stops at the leftover ".5"
+    {"integer_fraction", "%%MatrixMarket matrix coordinate integer general\n2 2 2\n1 1 1.5\n"
+                         "2 2 3\n"},
+    // format and symmetry are compared after lowering them
+    {"mixed_case_format", "%%MatrixMarket matrix COORDINATE real General\n2 2 1\n1 2 3\n"},
+};
+
+// Input both readers must reject.
+const char* kRejected[][2] = {
+    {"field_double", "%%MatrixMarket matrix coordinate double general\n1 1 1\n1 1 1\n"},
+    {"object_case", "%%MatrixMarket Matrix coordinate real general\n1 1 1\n1 1 1\n"},
+    {"field_case", "%%MatrixMarket matrix coordinate Real general\n1 1 1\n1 1 1\n"},
 };
 
 }  // namespace
@@ -43,6 +56,26 @@ int main() {
     fails += !same;
     std::printf("{\"case\": \"%s\", \"same\": %d, \"nnz_ref\": %d, \"nnz\": %d}\n", c[0], int(same),
                 int(R.nnz()), G.nnz());
+  }
+  for (auto& c : kRejected) {
+    std::istringstream s1(c[1]), s2(c[1]);
+    bool ref_threw = false, ours_threw = false;
+    try {
+      mtl::compressed2D<double> R;
+      mtl::io::matrix_market_istream mm(s1);
+      mm >> R;
+    } catch (...) {
+      ref_threw = true;
+    }
+    try {
+      mtlgpu::io::read_matrix_market(s2);
+    } catch (const mtlgpu::io::format_error&) {
+      ours_threw = true;
+    }
+    const bool same = ref_threw && ours_threw;
+    fails += !same;
+    std::printf("{\"case\": \"%s\", \"same\": %d, \"rejected_ref\": %d, \"rejected\": %d}\n",
+                c[0], int(same), int(ref_threw), int(ours_threw));
   }
   return fails ? 1 : 0;
 }

@@ -51,11 +51,23 @@ def test_symmetric_skew_pattern_duplicates_array(tmp_path):
 
 
 def test_rejected_input(tmp_path):
+    # rejected as the reference's reader rejects them (the header's object and
+    # field are compared as written; there is no 'double' field)
     for text in ("%%MatrixMarket matrix coordinate complex general\n1 1 1\n1 1 1 0\n",
                  "%%NotMarket matrix coordinate real general\n1 1 1\n1 1 1\n",
-                 "%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1\n"):
+                 "%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1\n",
+                 "%%MatrixMarket matrix coordinate double general\n1 1 1\n1 1 1\n",
+                 "%%MatrixMarket Matrix coordinate real general\n1 1 1\n1 1 1\n",
+                 "%%MatrixMarket matrix coordinate Real general\n1 1 1\n1 1 1\n"):
         rc, err = read(write(tmp_path, "bad.mtx", text))
         assert rc == 1 and err
+
+
+def test_integer_entries_read_as_integers(tmp_path):
+    # "1.5" in an integer file: 1 is read, and the reader stops at ".5"
+    rc, A = read(write(tmp_path, "i.mtx", "%%MatrixMarket matrix coordinate integer general\n"
+                                          "2 2 2\n1 1 1.5\n2 2 3\n"))
+    assert rc == 0 and A["starts"] == [0, 1, 1] and A["data"] == [1]
 
 
 def test_same_as_reference_reader():
@@ -64,7 +76,7 @@ def test_same_as_reference_reader():
         pytest.skip("built only where the MTL4 headers are present")
     p = subprocess.run([exe], capture_output=True, text=True)
     lines = [json.loads(l) for l in p.stdout.splitlines()]
-    assert p.returncode == 0 and len(lines) == 7 and all(l["same"] for l in lines)
+    assert p.returncode == 0 and len(lines) == 12 and all(l["same"] for l in lines), lines
 
 
 @pytest.mark.gpu
