@@ -285,49 +285,69 @@ def _local_ms(fn, reps, stream):
     return e0.elapsed_time(e1) / reps, out
 
 
-def batched_workload(M, ctx, stream):
+def batched_workload(M, ctx, stream, peak):
     """512 independent random-graph Laplacians (n log-uniform in [1e3, 65536],
     average degree U[8, 32], shift 1e-2 mean degree, seed 3), b ~ N(0,1):
-    one batched PCG to 1e-8 with Jacobi and IC(0), in FP64 and with FP32 inner
-    solves refined in FP64."""
+    batched PCG to 1e-8, FP64 and FP32 inner solves refined in FP64.  Jacobi,
+    and IC(0) applied by JACOBI_K Jacobi iterations per triangle, run as one
+    persistent launch (clusters taking systems from a work queue, shape
+    autotuned on these systems); IC(0) with exact triangular solves runs the
+    level-scheduled path.  Roofline: per system, iterations x (SpMV bytes +
+    10 n vector words), summed, over the solve time."""
     systems, (n, rp, ci, v, off) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2, seed=3)
     b = M.normal(n, 3)
     dA = M.Csr(ctx, rp, ci, v)
     db, dx, dz = ctx.to_device(b), ctx.array(n), ctx.to_device(np.zeros(n))
-    out = {"systems": 512, "n": int(n), "nnz": int(len(ci)), "rtol": 1e-8, "dtype": "f64"}
-    for pc in ("diagonal", "ic0"):
-        P = M.Pc(dA, pc)
+    ns = np.diff(off).astype(np.int64)
+    nnzs = np.array([len(sy[2]) for sy in systems], np.int64)
+    out = {"systems": 512, "n": int(n), "nnz": int(len(ci)), "rtol": 1e-8}
+
+    def run_case(P, mode, wsize):
+        kw = dict(rtol=1e-8, max_iter=5000)
+        if mode == "mixed":
+            kw["mode"] = M.SOLVE_MIXED
 
         def run():
             ctx.xpay(dz, 0.0, dx)
-            st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=5000)
+            st, res = M.solve_batched(dA, P, off, dx, db, **kw)
             assert st == M.OK, st
             return res
         run()
         ms, res = _local_ms(run, 2, stream)
-        its = np.array([r.iterations for r in res[-1]])
-        rel = max(r.true_resid / r.norm_r0 for r in res[-1])
-        out[pc] = {"ms": ms, "iterations_max": int(its.max()),
-                   "iterations_mean": float(its.mean()), "max_true_rel_residual": rel}
-        P.close()
-        # FP32 inner solves with FP64 refinement per system
-        P = M.Pc(dA, pc, M.FP32)
+        its = np.array([r.iterations for r in res[-1]], np.int64)
+        word = wsize
+        per_it = nnzs * (4 + word) + 4 * (ns + 1) + 10 * word * ns
+        byt = float((its * per_it).sum())
+        rec = {"ms": ms, "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
+               "max_true_rel_residual": max(r.true_resid / r.norm_r0 for r in res[-1]),
+               "algorithmic_GB": byt / 1e9, "GBps": byt / ms / 1e6,
+               "hbm_frac": byt / ms / 1e6 / peak}
+        if mode == "mixed":
+            rec["outer_max"] = int(max(r.outer_iterations for r in res[-1]))
+        return rec
 
-        def run32():
-            ctx.xpay(dz, 0.0, dx)
-            st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=5000,
-                                      mode=M.SOLVE_MIXED)
-            assert st == M.OK, st
-            return res
-        run32()
-        ms, res = _local_ms(run32, 2, stream)
-        its = np.array([r.iterations for r in res[-1]])
-        rel = max(r.true_resid / r.norm_r0 for r in res[-1])
-        out[pc + "_fp32_refined"] = {
-            "ms": ms, "inner_iterations_max": int(its.max()),
-            "outer_max": int(max(r.outer_iterations for r in res[-1])),
-            "max_true_rel_residual": rel}
+    P = M.Pc(dA, "diagonal")
+    t0 = time.perf_counter()
+    choice = M.batched_autotune(dA, P, off, dx, db, rtol=1e-8, max_iter=5000)
+    out["autotune"] = {"ctas_per_large_system": (choice % 1000) // 100,
+                       "lanes_per_row": choice % 100,
+                       "single_cta_below_rows": choice // 1000,
+                       "seconds": time.perf_counter() - t0}
+    out["diagonal"] = run_case(P, "fp64", 8)
+    P.close()
+    P = M.Pc(dA, "diagonal", M.FP32)
+    out["diagonal_fp32_refined"] = run_case(P, "mixed", 4)
+    P.close()
+    for prec, key, mode, w in ((M.FP64, "ic0_jacobi", "fp64", 8),
+                               (M.FP32, "ic0_jacobi_fp32_refined", "mixed", 4)):
+        P = M.Pc(dA, "ic0", prec)
+        P.set_jacobi_sweeps(JACOBI_K)
+        out[key] = run_case(P, mode, w)
+        out[key]["jacobi_iterations_per_triangle"] = JACOBI_K
         P.close()
+    P = M.Pc(dA, "ic0")
+    out["ic0_exact_sweeps"] = run_case(P, "fp64", 8)
+    P.close()
     dA.close()
     return out
 
@@ -646,7 +666,7 @@ def main():
     A3 = b3 = None
     if world == 1 and not args.no_extras:
         A3, b3, line["config3"] = config3_workload(M, ctx, timed, solver, spmv_stats, peak)
-        line["batched"] = batched_workload(M, ctx, stream)
+        line["batched"] = batched_workload(M, ctx, stream, peak)
         line["differentiable_solve"] = adjoint_workload(M, ctx, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if A3 is None:

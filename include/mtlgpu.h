@@ -188,8 +188,11 @@ mtlgpu_status mtlgpu_csr_create_transpose(mtlgpu_csr* A, mtlgpu_csr** out);
 mtlgpu_status mtlgpu_csr_values_grad(mtlgpu_csr* A, const double* d_lambda, const double* d_x,
                                      double* d_grad);
 
-/* Choose SpMV row-bin thresholds by timing the candidates on this matrix
- * (kept on the handle; reported in *h_choice when non-NULL). */
+/* Choose the SpMV layout of this matrix by timing the bit-exact candidates
+ * on it (CUDA events, 20 products each): SELL-32 where its padding is at most
+ * 2 nnz, and the CSR-stream row blocks.  The fastest is kept on the handle;
+ * *h_choice (when non-NULL) receives 2 (SELL-32) or 0 (CSR-stream).  No
+ * counterpart in the reference (the layout behind mat_vec_mult.hpp:620-689). */
 mtlgpu_status mtlgpu_csr_autotune(mtlgpu_csr* A, int* h_choice);
 
 /* y = alpha * A * x + beta * y.  With (alpha, beta) = (1, 0), (1, 1), (-1, 1)
@@ -331,11 +334,31 @@ void mtlgpu_iter_params_default(mtlgpu_iter_params* p);
  * per system, as mtlgpu_solve does for one system; iterations then counts
  * inner iterations and outer_iterations the refinement steps.  h_results
  * (host, count entries) receives each system's iteration state; the call
- * returns MTLGPU_MAX_ITER when any system stopped on max_iter. */
+ * returns MTLGPU_MAX_ITER when any system stopped on max_iter.
+ * Execution: with P NULL, diagonal, or ic_0 / ilu_0 applied by Jacobi
+ * iterations (mtlgpu_pc_set_jacobi_sweeps), the whole solve -- refinement
+ * included -- is ONE persistent kernel launch: thread-block clusters take
+ * systems from a work queue (largest first) and each runs its system's
+ * iterations, so a converged system releases its cluster at once.  With the
+ * exact triangular solves of ic_0 / ilu_0 the iterations of all systems run
+ * together, one level-scheduled sweep over the block-diagonal factors. */
 mtlgpu_status mtlgpu_solve_batched(int method, mtlgpu_csr* A, mtlgpu_pc* P, int count,
                                    const int32_t* h_offsets, double* d_x, const double* d_b,
                                    const mtlgpu_iter_params* params,
                                    mtlgpu_iter_result* h_results);
+/* Tunes mtlgpu_solve_batched for these systems: times short solves (at most
+ * 8 iterations, one refinement step; x is not modified) for every candidate
+ * of CTAs per large system (4, 8: the thread-block cluster that runs it),
+ * lanes per matrix row (4, 8, 16), and the row count below which a system is
+ * solved by a single CTA (0, 8192, 32768), and keeps the fastest on A.
+ * *h_choice = 1000 * rows + 100 * CTAs + lanes.  Applies to the persistent-launch path
+ * (P NULL, diagonal, or factors applied by Jacobi iterations); other
+ * preconditioners return MTLGPU_NOT_SUPPORTED.  No counterpart in the
+ * reference. */
+mtlgpu_status mtlgpu_batched_autotune(mtlgpu_csr* A, mtlgpu_pc* P, int count,
+                                      const int32_t* h_offsets, const double* d_x,
+                                      const double* d_b, const mtlgpu_iter_params* params,
+                                      int* h_choice);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -14,6 +14,8 @@
 // deterministic.  A system that has stopped keeps its x; its CTAs return at
 // once.  The host checks a stopped-systems counter every few iterations.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -254,6 +256,19 @@ __global__ void __launch_bounds__(kBlock)
 
 }  // namespace
 
+// Rejects a row of system s referencing a column outside system s.
+mtlgpu_status batch_check(Csr* A, int count, const int32_t* h_off) {
+  Ctx* ctx = A->ctx;
+  int32_t* d_off = nullptr;
+  MTLGPU_TRY(dalloc(ctx, &d_off, count + 1));
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(d_off, h_off, sizeof(int32_t) * (count + 1),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+  batch_check_kernel<<<count, kBlock, 0, ctx->stream>>>(d_off, A->d_rp, A->d_ci, ctx->d_error);
+  ctx->launches++;
+  dfree(ctx, d_off);
+  return take_device_error(ctx);
+}
+
 // FP32 inner batched PCG with FP64 iterative refinement, per system: the
 // outer loop (FP64 residual, stopping test, x += ||r|| d) runs for all
 // systems at once, and systems that have converged sit out.
@@ -407,6 +422,23 @@ mtlgpu_status solve_batched_impl(int method, Csr* A, Pc* P, int count, const int
   if (h_off[0] != 0 || h_off[count] != A->n_rows) return MTLGPU_INCOMPATIBLE_SIZE;
   for (int s = 0; s < count; ++s)
     if (h_off[s + 1] < h_off[s]) return MTLGPU_INVALID_ARG;
+  if (batched_cluster_supported(P)) {
+    MTLGPU_TRY(batch_check(A, count, h_off));
+    int cs = A->batch_cs, g = A->batch_g;
+    int small = A->batch_small;
+    // MTLGPU_BATCH_SHAPE="CTAs,lanes[,small rows]" overrides the tuned shape
+    // (testing)
+    if (const char* m = std::getenv("MTLGPU_BATCH_SHAPE")) {
+      int c2 = 0, g2 = 0, s2 = -1;
+      const int k = std::sscanf(m, "%d,%d,%d", &c2, &g2, &s2);
+      if (k >= 2 && (c2 == 1 || c2 == 2 || c2 == 4 || c2 == 8) &&
+          (g2 == 4 || g2 == 8 || g2 == 16 || g2 == 32)) {
+        cs = c2, g = g2;
+        if (k == 3 && s2 >= 0) small = s2;
+      }
+    }
+    return solve_batched_cluster(A, P, count, h_off, d_x, d_b, prm, res, cs, g, small, nullptr);
+  }
   if (prm->mode == MTLGPU_SOLVE_MIXED_REFINED)
     return solve_batched_mixed(A, P, count, h_off, d_x, d_b, prm, res);
   const int n = A->n_rows;
@@ -518,7 +550,57 @@ mtlgpu_status solve_batched_impl(int method, Csr* A, Pc* P, int count, const int
   return any_max ? MTLGPU_MAX_ITER : MTLGPU_OK;
 }
 
+// Times the persistent kernel's candidates -- CTAs per system (the cluster
+// size), lanes per row, and the row count below which a system is solved by
+// one CTA -- on the caller's systems: a short solve each (at most 8
+// iterations, one refinement step), from a copy of x.  Keeps the fastest on A.
+mtlgpu_status batched_autotune_impl(Csr* A, Pc* P, int count, const int32_t* h_off,
+                                           const double* d_x, const double* d_b,
+                                           const mtlgpu_iter_params* prm, int* choice) {
+  Ctx* ctx = A->ctx;
+  if (count <= 0 || !h_off || !d_x || !d_b || !prm) return MTLGPU_INVALID_ARG;
+  if (h_off[0] != 0 || h_off[count] != A->n_rows) return MTLGPU_INCOMPATIBLE_SIZE;
+  if (!batched_cluster_supported(P)) return MTLGPU_NOT_SUPPORTED;
+  double* x = nullptr;
+  MTLGPU_TRY(dalloc(ctx, &x, A->n_rows));
+  std::vector<mtlgpu_iter_result> res(count);
+  mtlgpu_iter_params p = *prm;
+  p.max_iter = std::min(p.max_iter, 8);
+  p.max_outer = 1;
+  p.h_interrupt = nullptr;
+  float best_ms = 1e30f;
+  int best_cs = A->batch_cs, best_g = A->batch_g, best_small = A->batch_small;
+  for (int cs : {4, 8})
+    for (int g : {4, 8, 16})
+      for (int small : {0, 8192, 32768}) {
+        cudaMemcpyAsync(x, d_x, sizeof(double) * A->n_rows, cudaMemcpyDeviceToDevice,
+                        ctx->stream);
+        float ms = 0;
+        mtlgpu_status st = solve_batched_cluster(A, P, count, h_off, x, d_b, &p, res.data(), cs,
+                                                 g, small, &ms);
+        if (st != MTLGPU_OK && st != MTLGPU_MAX_ITER) {
+          dfree(ctx, x);
+          return st;
+        }
+        if (ms < best_ms) best_ms = ms, best_cs = cs, best_g = g, best_small = small;
+      }
+  A->batch_cs = best_cs;
+  A->batch_g = best_g;
+  A->batch_small = best_small;
+  dfree(ctx, x);
+  if (choice) *choice = best_small * 1000 + best_cs * 100 + best_g;
+  return take_device_error(ctx);
+}
+
 }  // namespace mtlgpu
+
+extern "C" mtlgpu_status mtlgpu_batched_autotune(mtlgpu_csr* A, mtlgpu_pc* P, int count,
+                                                 const int32_t* h_offsets, const double* d_x,
+                                                 const double* d_b,
+                                                 const mtlgpu_iter_params* params, int* h_choice) {
+  if (!A || (P && P->A != A)) return MTLGPU_INVALID_ARG;
+  return mtlgpu::batched_autotune_impl(A, P, count, h_offsets, d_x, d_b, params, h_choice);
+}
 
 extern "C" mtlgpu_status mtlgpu_solve_batched(int method, mtlgpu_csr* A, mtlgpu_pc* P, int count,
                                               const int32_t* h_offsets, double* d_x,

@@ -558,7 +558,10 @@ mtlgpu_status mtlgpu_solve_host(int method, mtlgpu_csr* A, mtlgpu_pc* P, double*
 
 mtlgpu_status mtlgpu_csr_autotune(mtlgpu_csr* A, int* choice) {
   if (!A) return MTLGPU_INVALID_ARG;
-  if (choice) *choice = A->uniform ? A->uniform_group : -1;
+  int c = 0;
+  float ms[3];
+  MTLGPU_TRY(csr_autotune_spmv(A, &c, ms));
+  if (choice) *choice = c;
   return MTLGPU_OK;
 }
 

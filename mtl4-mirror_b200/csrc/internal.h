@@ -100,6 +100,11 @@ struct Csr {
   int n_blk = 0;
   int spmv_kernel = 0;             // 0 = CSR-stream, 1 = row-binned groups, 2 = SELL-32
   Sell sell;                       // SELL-32 copy (spmv_kernel == 2)
+  // batched solves: CTAs per system (cluster size), lanes per row, and the
+  // row count below which a system is solved by one CTA; picked by
+  // mtlgpu_batched_autotune
+  int batch_cs = 4, batch_g = 8, batch_small = 4096;
+  void* batch_work = nullptr;      // cached batched configuration (batched_cluster.cu)
   // transpose (built on demand for A^T x)
   int32_t* d_trp = nullptr;
   int32_t* d_tci = nullptr;
@@ -221,6 +226,15 @@ struct SpmvArgs {
 template <typename T>
 mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args);
 mtlgpu_status spmv_transposed_launch(Csr* A, const double* x, double* y);
+mtlgpu_status csr_autotune_spmv(Csr* A, int* choice, float* ms);
+
+// Batched PCG in one persistent cluster launch (batched_cluster.cu).
+bool batched_cluster_supported(const Pc* P);
+void release_batch_work(Csr* A, const Pc* only_P);
+mtlgpu_status solve_batched_cluster(Csr* A, Pc* P, int count, const int32_t* h_off, double* d_x,
+                                    const double* d_b, const mtlgpu_iter_params* prm,
+                                    mtlgpu_iter_result* res, int cs, int g, int small_rows,
+                                    float* ms_out);
 
 // Sweeps (sweep.cu): out must be prefilled with the sentinel when
 // prefilled == true; otherwise the launcher fills it first.

@@ -571,6 +571,71 @@ mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args) {
 }
 
 template mtlgpu_status spmv_launch<double>(Csr*, const double*, double*, const SpmvArgs&);
+
+// Times the bit-exact SpMV layouts on this matrix (SELL-32 where its padding
+// is at most 2 nnz, CSR-stream) with CUDA events, 20 products each after a
+// warm-up, and keeps the fastest on the handle.  *choice: the kernel kept
+// (0 CSR-stream, 2 SELL-32); ms[k]: its mean time per product (-1: not a
+// candidate).
+mtlgpu_status csr_autotune_spmv(Csr* A, int* choice, float* ms) {
+  Ctx* ctx = A->ctx;
+  ms[0] = ms[1] = ms[2] = -1.f;
+  if (A->n_rows == 0 || A->nnz == 0) {
+    *choice = A->spmv_kernel;
+    return MTLGPU_OK;
+  }
+  if (A->spmv_kernel != 2 && !A->sell.d_slice_ptr) {
+    std::vector<int32_t> h_rp(A->n_rows + 1);
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h_rp.data(), A->d_rp, sizeof(int32_t) * (A->n_rows + 1),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const long long padded = sell_padded_entries(A->n_rows, h_rp.data(), 0);
+    if (padded <= 2ll * A->nnz && padded < (1ll << 31))
+      MTLGPU_TRY(sell_build(ctx, A->n_rows, A->d_rp, A->d_ci, A->d_v, 0, true, false, false,
+                            false, &A->sell));
+  }
+  double *x = nullptr, *y = nullptr;
+  MTLGPU_TRY(dalloc(ctx, &x, A->n_cols));
+  MTLGPU_TRY(dalloc(ctx, &y, A->n_rows));
+  MTLGPU_TRY_CUDA(ctx, cudaMemsetAsync(x, 0, sizeof(double) * A->n_cols, ctx->stream));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int keep = A->spmv_kernel;
+  int best = keep;
+  float best_ms = 1e30f;
+  SpmvArgs plain;
+  for (int k : {2, 0}) {
+    if (k == 2 && !A->sell.d_slice_ptr) continue;
+    A->spmv_kernel = k;
+    mtlgpu_status st = spmv_launch<double>(A, x, y, plain);
+    cudaEventRecord(e0, ctx->stream);
+    for (int r = 0; r < 20 && st == MTLGPU_OK; r++) st = spmv_launch<double>(A, x, y, plain);
+    cudaEventRecord(e1, ctx->stream);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (st != MTLGPU_OK) {
+      A->spmv_kernel = keep;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      dfree(ctx, x);
+      dfree(ctx, y);
+      return st;
+    }
+    ms[k] = t / 20;
+    if (ms[k] < best_ms) best_ms = ms[k], best = k;
+  }
+  A->spmv_kernel = best;
+  release_workspaces(A, nullptr);  // solver graphs captured the previous kernel
+  if (best != 2 && A->sell.d_slice_ptr) sell_free(ctx, &A->sell);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(ctx, x);
+  dfree(ctx, y);
+  *choice = best;
+  return take_device_error(ctx);
+}
 template mtlgpu_status spmv_launch<float>(Csr*, const float*, float*, const SpmvArgs&);
 
 mtlgpu_status spmv_transposed_launch(Csr* A, const double* x, double* y) {

@@ -392,6 +392,18 @@ def solve_batched(A, P, offsets, x, b, **kw):
     return st, list(res)
 
 
+def batched_autotune(A, P, offsets, x, b, **kw):
+    """mtlgpu_batched_autotune: times the batched kernel's shapes on these
+    systems and keeps the fastest on A; returns 1000 * (rows below which one
+    CTA solves a system) + 100 * (CTAs per larger system) + lanes per row."""
+    off = np.ascontiguousarray(offsets, np.int32)
+    prm = make_params(**kw)
+    c = C.c_int()
+    check(_lib().mtlgpu_batched_autotune(A.h, P.h if P else None, len(off) - 1, _p(off), x.ptr,
+                                         b.ptr, C.byref(prm), C.byref(c)), "batched_autotune")
+    return c.value
+
+
 def solve_host(method, A, P, x, b, **kw):
     """Same with host numpy x (updated in place) and b."""
     hist = np.zeros(2 * kw.get("max_iter", 1000) + 8)

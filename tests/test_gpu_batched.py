@@ -78,3 +78,105 @@ def test_batched_mixed_refinement_reaches_fp64_tolerance(M, ctx, pc):
         assert res[s].error == 0 and res[s].outer_iterations >= 1
         assert tr <= 1e-8, (s, tr)
         assert abs(res[s].true_resid / np.linalg.norm(b[a:e]) - tr) <= 1e-10
+
+
+def _batch_env(shape):
+    import os
+    old = os.environ.get("MTLGPU_BATCH_SHAPE")
+    os.environ["MTLGPU_BATCH_SHAPE"] = shape
+    return old
+
+
+def _restore(old):
+    import os
+    if old is None:
+        os.environ.pop("MTLGPU_BATCH_SHAPE", None)
+    else:
+        os.environ["MTLGPU_BATCH_SHAPE"] = old
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", ["1,8", "2,4", "4,16", "8,32", "8,8,0", "4,8,1500",
+                                   "8,16,100000"])
+def test_batched_cluster_shapes_match_each_system(M, ctx, restate, shape):
+    # every (CTAs per system, lanes per row, rows below which one CTA solves
+    # a system) shape of the persistent launch gives each system the
+    # reference's iteration count
+    systems, (n, rp, ci, v, off) = M.graph_batch(9, 100, 3000, 8.0, 32.0, 1e-2, seed=9)
+    b = M.normal(n, 2)
+    dA = M.Csr(ctx, rp, ci, v)
+    P = M.Pc(dA, "diagonal")
+    dx, db = ctx.to_device(np.zeros(n)), ctx.to_device(b)
+    old = _batch_env(shape)
+    try:
+        st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=2000)
+    finally:
+        _restore(old)
+    assert st == M.OK
+    x = dx.download()
+    for s, A_s in enumerate(systems):
+        a, e = off[s], off[s + 1]
+        ref = restate.solve("cg", "diagonal", A_s, b[a:e], rtol=1e-8, max_iter=2000)
+        assert abs(res[s].iterations - ref["iterations"]) <= 2, (s, res[s].iterations,
+                                                                ref["iterations"])
+        tr = np.linalg.norm(b[a:e] - M.csr_mult(A_s, x[a:e])) / np.linalg.norm(b[a:e])
+        assert tr <= 3e-8 and rel_err(x[a:e], ref["x"]) <= 1e-6
+        assert res[s].kernel_launches == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+@pytest.mark.parametrize("pc", ["ic0", "ilu0"])
+def test_batched_jacobi_applied_factors(M, ctx, mode, pc):
+    # factors applied by Jacobi iterations: the persistent launch, FP64 or FP32
+    # inner solves with FP64 refinement; each system reaches 1e-8 (true residual)
+    systems, (n, rp, ci, v, off) = M.graph_batch(10, 200, 4000, 8.0, 32.0, 1e-2, seed=4)
+    b = M.normal(n, 3)
+    dA = M.Csr(ctx, rp, ci, v)
+    P = M.Pc(dA, pc, M.FP32 if mode == "mixed" else M.FP64)
+    P.set_jacobi_sweeps(2)
+    dx, db = ctx.to_device(np.zeros(n)), ctx.to_device(b)
+    kw = dict(rtol=1e-8, max_iter=4000)
+    if mode == "mixed":
+        kw["mode"] = M.SOLVE_MIXED
+    st, res = M.solve_batched(dA, P, off, dx, db, **kw)
+    assert st == M.OK
+    x = dx.download()
+    for s, A_s in enumerate(systems):
+        a, e = off[s], off[s + 1]
+        tr = np.linalg.norm(b[a:e] - M.csr_mult(A_s, x[a:e])) / np.linalg.norm(b[a:e])
+        assert res[s].error == 0 and tr <= (1e-8 if mode == "mixed" else 3e-8), (s, tr)
+
+
+@pytest.mark.gpu
+def test_batched_autotune(M, ctx, restate):
+    systems, (n, rp, ci, v, off) = M.graph_batch(12, 500, 6000, 8.0, 32.0, 1e-2, seed=6)
+    b = M.normal(n, 4)
+    dA = M.Csr(ctx, rp, ci, v)
+    P = M.Pc(dA, "diagonal")
+    x0 = M.uniform(n, 8)
+    dx, db = ctx.to_device(x0), ctx.to_device(b)
+    choice = M.batched_autotune(dA, P, off, dx, db, rtol=1e-8, max_iter=2000)
+    assert choice // 1000 in (0, 8192, 32768)
+    assert (choice % 1000) // 100 in (4, 8) and choice % 100 in (4, 8, 16)
+    assert np.array_equal(dx.download(), x0)      # the caller's x is not touched
+    dx.upload(np.zeros(n))
+    st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=2000)
+    assert st == M.OK
+    for s, A_s in enumerate(systems):
+        a, e = off[s], off[s + 1]
+        ref = restate.solve("cg", "diagonal", A_s, b[a:e], rtol=1e-8, max_iter=2000)
+        assert abs(res[s].iterations - ref["iterations"]) <= 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("A_fn", [lambda M: M.laplacian3d(40), lambda M: M.random_graph(20000, 20.0, 1e-2, 2)])
+def test_spmv_autotune_keeps_results(M, ctx, restate, A_fn):
+    A = A_fn(M)
+    dA = M.Csr(ctx, *A[1:])
+    choice = dA.autotune()
+    assert choice in (0, 2)
+    x = M.uniform(A[0], 3)
+    dx, dy = ctx.to_device(x), ctx.array(A[0])
+    dA.spmv(dx, dy)
+    assert np.array_equal(dy.download(), restate.spmv(A, x))
