@@ -50,7 +50,10 @@ mtlgpu_status ctx_init(Ctx* ctx) {
   MTLGPU_TRY_CUDA(ctx, cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount,
                                               ctx->device));
   if (const char* m = std::getenv("MTLGPU_SWEEP_BLOCKS_PER_SM")) ctx->sweep_blocks_per_sm = std::atoi(m);
-  if (const char* m = std::getenv("MTLGPU_SWEEP")) ctx->part_sweeps = std::strcmp(m, "part") == 0;
+  if (const char* m = std::getenv("MTLGPU_SWEEP")) {
+    if (!std::strcmp(m, "part")) ctx->part_sweeps = 1;
+    if (!std::strcmp(m, "ticket")) ctx->part_sweeps = 0;
+  }
   if (const char* m = std::getenv("MTLGPU_PART_ROWS")) ctx->part_rows = std::atoi(m);
   MTLGPU_TRY(dalloc(ctx, &ctx->d_partials, (size_t)kMaxPartials * kPartialWidth));
   MTLGPU_TRY(dalloc(ctx, &ctx->d_counters, kNumCounters));

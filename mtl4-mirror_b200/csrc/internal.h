@@ -38,9 +38,10 @@ struct Ctx {
   // less for L2; 2 measured best on B200).  Benchmark override:
   // MTLGPU_SWEEP_BLOCKS_PER_SM.
   int sweep_blocks_per_sm = 2;
-  // Partitioned sweeps (part_sweep.cu): built at preconditioner creation when
-  // enabled (MTLGPU_SWEEP=part|ticket), rows per part (MTLGPU_PART_ROWS).
-  bool part_sweeps = false;
+  // Partitioned sweeps (part_sweep.cu), built at preconditioner creation:
+  // 2 = automatic (factors with narrow levels), 1 = always (MTLGPU_SWEEP=part),
+  // 0 = never (MTLGPU_SWEEP=ticket); rows per part (MTLGPU_PART_ROWS).
+  int part_sweeps = 2;
   int part_rows = 16384;
 };
 

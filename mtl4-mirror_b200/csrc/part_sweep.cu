@@ -56,6 +56,10 @@ using namespace dev;
 
 namespace {
 
+// Automatic selection: partitioned sweeps for factors with at most this many
+// rows per level.
+constexpr int kAutoRowsPerLevel = 1024;
+
 constexpr int kPartThreads = 256;   // consumer threads: rows per block at most
 constexpr int kProducers = 64;      // producer threads (two warps): copies and gathers
 constexpr int kCtaThreads = kPartThreads + kProducers;
@@ -672,9 +676,13 @@ bool part_plan_host(const PartInput& in, HostPart* out) {
 // Built at preconditioner creation (outside any stream capture).
 mtlgpu_status part_plan_build(Ctx* ctx, SweepPlan* S, bool with_fp32) {
   part_plan_free(ctx, S);
-  if (!ctx->part_sweeps) return MTLGPU_OK;
   const int n = S->n;
-  if (n == 0) return MTLGPU_OK;
+  if (n == 0 || ctx->part_sweeps == 0) return MTLGPU_OK;
+  // automatic choice: the partitioned sweep where levels are narrow (few rows
+  // per level, long dependency chains: 2-D grids, where it measured 16 %
+  // faster); the level-ordered ticket sweep where levels are wide (3-D grids)
+  if (ctx->part_sweeps == 2 && (S->n_levels == 0 || n / S->n_levels > kAutoRowsPerLevel))
+    return MTLGPU_OK;
 
   // host copies of the level-ordered plan
   std::vector<int32_t> lp(S->n_levels + 1), row_of(n), rp(n + 1), ci(S->nnz_off);

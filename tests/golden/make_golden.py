@@ -6,6 +6,7 @@ Run in a checkout where the reference tree is present (it is compiled by
     python tests/golden/make_golden.py            # small cases (seconds)
     python tests/golden/make_golden.py --cfg2     # + the 128^3 solve (about a minute)
     python tests/golden/make_golden.py --cfg3     # + the 96^3 27-point BiCGSTAB solve
+    python tests/golden/make_golden.py --cfg5     # + the 512^2 CPU adjoint (gradients)
 
 Every array stored here is an output of the reference's own code path
 (laplacian_setup, compressed2D SpMV, ic_0 / ilu_0 factors, solve(P, x),
@@ -34,10 +35,53 @@ def put_csr(out, key, A):
     out[key + "_rp"], out[key + "_ci"], out[key + "_v"] = A[1], A[2], A[3]
 
 
+def fv_source(N):
+    """The Gaussian source of the differentiable-solve workload."""
+    c = (np.arange(N) + 0.5) / N - 0.5
+    X, Y = np.meshgrid(c, c, indexing="ij")
+    return np.exp(-(X ** 2 + Y ** 2) / (2 * 0.1 ** 2)).ravel()
+
+
+CFG5_DIRECTIONS = 64
+
+
+def cfg5(R, out):
+    """Config 5: the FP64 CPU adjoint by the reference itself.  512 x 512
+    finite-volume operator (sigma 1, 8-cell correlation, seed 4), b the
+    Gaussian source, L = 1/2 ||x - x_target||^2 with x_target = x + 0.01 N(0,1)
+    (seed 44), so dL/dx = -0.01 N(0,1) at the solution.  itl::cg + ic_0 to
+    1e-13 for x = A^-1 b and for lambda = A^-T dL/dx; dL/db = lambda and
+    dL/dvals = -lambda_i x_j on A's pattern.  Stored: their projections on
+    64 seeded random directions (N(0,1), seeds 1000 + m for b, 2000 + m for
+    the values), their norms, and 1024 sampled entries."""
+    A = M.fv2d(512, 1.0, 8.0, 4)
+    n, rp, ci, v = A
+    b = fv_source(512)
+    rf = R.solve("cg", "ic0", A, b, rtol=1e-13, max_iter=20000)
+    g = -0.01 * M.normal(n, 44)
+    ra = R.solve("cg", "ic0", A, g, rtol=1e-13, max_iter=20000)
+    assert rf["err"] == 0 and ra["err"] == 0, (rf["err"], ra["err"])
+    x, lam = rf["x"], ra["x"]
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    G = -lam[rows] * x[ci]
+    pb = np.array([lam @ M.normal(n, 1000 + m) for m in range(CFG5_DIRECTIONS)])
+    pv = np.array([G @ M.normal(len(ci), 2000 + m) for m in range(CFG5_DIRECTIONS)])
+    rng = np.random.default_rng(5)
+    ib = rng.choice(n, 1024, replace=False)
+    iv = rng.choice(len(ci), 1024, replace=False)
+    out["cfg5_proj_b"], out["cfg5_proj_vals"] = pb, pv
+    out["cfg5_norms"] = np.array([np.linalg.norm(lam), np.linalg.norm(G), np.linalg.norm(x)])
+    out["cfg5_idx_b"], out["cfg5_lambda_sample"] = ib.astype(np.int64), lam[ib]
+    out["cfg5_idx_vals"], out["cfg5_grad_vals_sample"] = iv.astype(np.int64), G[iv]
+    out["cfg5_x_sample"] = x[ib]
+    out["cfg5_iters"] = np.array([rf["iterations"], ra["iterations"]])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
     ap.add_argument("--cfg3", action="store_true")
+    ap.add_argument("--cfg5", action="store_true")
     args = ap.parse_args()
     R = O.Reference()
     S = O.Restatement()
@@ -135,11 +179,13 @@ def main():
         out["cfg3_iters"] = np.array([rr["iterations"], rr["err"]])
         out["cfg3_hist"] = rr["history"]
         out["cfg3_b_sum"] = np.array([b.sum(), np.linalg.norm(b)])
+    if args.cfg5:
+        cfg5(R, out)
     old = os.path.join(HERE, "golden.npz")
     if os.path.exists(old):
         prev = np.load(old)
         for k in prev.files:
-            if k.startswith(("cfg2_", "cfg3_")) and k not in out:
+            if k.startswith(("cfg2_", "cfg3_", "cfg5_")) and k not in out:
                 out[k] = prev[k]
 
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
