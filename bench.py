@@ -438,6 +438,50 @@ def profile_case(case, grid, launches):
     print(json.dumps({"profile_case": case, "grid": grid, "launches": launches}))
 
 
+def sweep_scan():
+    """Exact IC(0) lower sweep (level-ordered ticket kernel) on N^3 7-point
+    Laplacians, N = 64 .. 192: time per sweep with CUDA events (20 sweeps
+    after 3 warm-ups), levels (3N - 2) and rows per level.  A least-squares
+    line time/level = hop + row_cost * rows/level splits the per-level cost
+    into the dependency hop and the row work."""
+    import torch
+    import mtlgpu as M
+    os.environ["MTLGPU_SWEEP"] = "ticket"
+    ctx = M.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device="cuda:0")
+    rows = []
+    for N in (64, 96, 128, 160, 192):
+        A = M.laplacian3d(N)
+        n = A[0]
+        dA = M.Csr(ctx, *A[1:])
+        for prec, dt, name in ((M.FP64, np.float64, "f64"), (M.FP32, np.float32, "f32")):
+            P = M.Pc(dA, "ic0", prec)
+            r, z = ctx.to_device(np.ones(n, dt)), ctx.array(n, dt)
+            for _ in range(3):
+                P.sweep(M.LOWER, r, z)
+            ctx.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(20):
+                P.sweep(M.LOWER, r, z)
+            e1.record(stream)
+            ctx.synchronize()
+            ms = e0.elapsed_time(e1) / 20
+            lev = P.factor_info(M.LOWER)[1]
+            rec = {"N": N, "prec": name, "n": n, "levels": lev, "rows_per_level": n / lev,
+                   "sweep_ms": ms, "us_per_level": 1e3 * ms / lev}
+            rows.append(rec)
+            print(json.dumps(rec), flush=True)
+            P.close()
+        dA.close()
+    for name in ("f64", "f32"):
+        pts = [(r["rows_per_level"], r["us_per_level"]) for r in rows if r["prec"] == name]
+        xs, ys = np.array([p[0] for p in pts]), np.array([p[1] for p in pts])
+        slope, hop = np.polyfit(xs, ys, 1)
+        print(json.dumps({"fit": name, "hop_us": hop, "us_per_1000_rows": 1e3 * slope}),
+              flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,11 +493,16 @@ def main():
                     help="skip the config-3, batched and differentiable-solve measurements")
     ap.add_argument("--profile-case",
                     choices=["spmv", "spmv32", "jacobi32", "sweep64", "sweep32", "mixed"])
+    ap.add_argument("--sweep-scan", action="store_true",
+                    help="per-level cost of the exact sweep on 64^3 .. 192^3 grids")
     ap.add_argument("--grid", type=int, default=64)
     ap.add_argument("--launches", type=int, default=3)
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case, args.grid, args.launches)
+        return
+    if args.sweep_scan:
+        sweep_scan()
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -40,7 +40,35 @@ const char* kRejected[][2] = {
 
 }  // namespace
 
-int main() {
+// With file arguments: compare both readers on each file and print the CSR
+// arrays of ours (one JSON line per file).
+int compare_files(int argc, char** argv) {
+  int fails = 0;
+  for (int a = 1; a < argc; ++a) {
+    mtl::compressed2D<double> R;
+    mtl::io::matrix_market_istream mm(argv[a]);
+    mm >> R;
+    mtlgpu::io::csr_matrix G = mtlgpu::io::read_matrix_market(std::string(argv[a]));
+    bool same = int(num_rows(R)) == G.n_rows && int(num_cols(R)) == G.n_cols &&
+                int(R.nnz()) == G.nnz();
+    for (int i = 0; same && i <= G.n_rows; ++i) same = int(R.ref_major()[i]) == G.starts[i];
+    for (int k = 0; same && k < G.nnz(); ++k)
+      same = int(R.ref_minor()[k]) == G.indices[k] && R.data[k] == G.data[k];
+    fails += !same;
+    std::printf("{\"file\": \"%s\", \"same\": %d, \"rows\": %d, \"cols\": %d, \"starts\": [",
+                argv[a], int(same), G.n_rows, G.n_cols);
+    for (size_t i = 0; i < G.starts.size(); ++i) std::printf("%s%d", i ? ", " : "", G.starts[i]);
+    std::printf("], \"indices\": [");
+    for (size_t i = 0; i < G.indices.size(); ++i) std::printf("%s%d", i ? ", " : "", G.indices[i]);
+    std::printf("], \"data\": [");
+    for (size_t i = 0; i < G.data.size(); ++i) std::printf("%s%.17g", i ? ", " : "", G.data[i]);
+    std::printf("]}\n");
+  }
+  return fails ? 1 : 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc > 1) return compare_files(argc, argv);
   int fails = 0;
   for (auto& c : kCases) {
     std::istringstream s1(c[1]), s2(c[1]);

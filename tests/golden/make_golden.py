@@ -7,6 +7,8 @@ Run in a checkout where the reference tree is present (it is compiled by
     python tests/golden/make_golden.py --cfg2     # + the 128^3 solve (about a minute)
     python tests/golden/make_golden.py --cfg3     # + the 96^3 27-point BiCGSTAB solve
     python tests/golden/make_golden.py --cfg5     # + the 512^2 CPU adjoint (gradients)
+    REFERENCE_ROOT=<MTL4 tree> python tests/golden/make_golden.py --mtx
+                                                  # + the reference's Matrix Market fixtures
 
 Every array stored here is an output of the reference's own code path
 (laplacian_setup, compressed2D SpMV, ic_0 / ilu_0 factors, solve(P, x),
@@ -77,11 +79,62 @@ def cfg5(R, out):
     out["cfg5_iters"] = np.array([rf["iterations"], ra["iterations"]])
 
 
+MTX_FIXTURES = ("bcsstk01", "bcspwr02", "jgl009", "plskz362", "dense_read")
+
+
+def mtx_fixtures(R, S, out):
+    """The real-valued Matrix Market files among the reference's test
+    fixtures (libs/numeric/mtl/test/matrix_market/): each is read by the
+    reference's own reader and by <mtlgpu/matrix_market.hpp> (tests/cpp/
+    mm_parity, which fails unless both give the same CSR arrays); stored are
+    the arrays and the reference's results on them: the SpMV of a seeded x
+    for every file, and for the SPD stiffness matrix bcsstk01 its IC(0) and
+    ILU(0) factors and its solves.  (mhd1280b is complex Hermitian and
+    outside the real-valued path; obstacle_small and square3 are not Matrix
+    Market files.)"""
+    import json
+    import subprocess
+    root = os.environ.get("REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("--mtx needs REFERENCE_ROOT (the MTL4 tree)")
+    d = os.path.join(root, "libs", "numeric", "mtl", "test", "matrix_market")
+    exe = os.path.join(ROOT, "tests", "cpp", "_build", "mm_parity")
+    for name in MTX_FIXTURES:
+        p = subprocess.run([exe, os.path.join(d, name + ".mtx")], capture_output=True, text=True)
+        rec = json.loads(p.stdout.splitlines()[-1])
+        assert p.returncode == 0 and rec["same"] == 1, name
+        rp = np.array(rec["starts"], np.int32)
+        ci = np.array(rec["indices"], np.int32)
+        v = np.array(rec["data"], np.float64)
+        rows, cols = rec["rows"], rec["cols"]
+        key = "mtx_" + name
+        out[key + "_rp"], out[key + "_ci"], out[key + "_v"] = rp, ci, v
+        out[key + "_shape"] = np.array([rows, cols])
+        x = M.uniform(cols, 7)
+        A = (rows, rp, ci, v)
+        out[key + "_x"] = x
+        out[key + "_spmv"] = R.spmv(A, x) if rows == cols else S.spmv(A, x)
+    # bcsstk01: factors and solves by the reference
+    A = (48, out["mtx_bcsstk01_rp"], out["mtx_bcsstk01_ci"], out["mtx_bcsstk01_v"])
+    L, U = R.ic0(A)
+    out["mtx_bcsstk01_ic0_L_v"], out["mtx_bcsstk01_ic0_U_v"] = L[3], U[3]
+    L, U = R.ilu0(A)
+    out["mtx_bcsstk01_ilu0_L_v"], out["mtx_bcsstk01_ilu0_U_v"] = L[3], U[3]
+    b = R.spmv(A, M.uniform(48, 1))
+    out["mtx_bcsstk01_b"] = b
+    its = []
+    for method, pc in (("cg", "ic0"), ("cg", "diagonal"), ("bicgstab", "ilu0")):
+        r = R.solve(method, pc, A, b, rtol=1e-10, max_iter=1000)
+        its.append([r["iterations"], r["err"]])
+    out["mtx_bcsstk01_iters"] = np.array(its)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
     ap.add_argument("--cfg3", action="store_true")
     ap.add_argument("--cfg5", action="store_true")
+    ap.add_argument("--mtx", action="store_true")
     args = ap.parse_args()
     R = O.Reference()
     S = O.Restatement()
@@ -181,11 +234,13 @@ def main():
         out["cfg3_b_sum"] = np.array([b.sum(), np.linalg.norm(b)])
     if args.cfg5:
         cfg5(R, out)
+    if args.mtx:
+        mtx_fixtures(R, S, out)
     old = os.path.join(HERE, "golden.npz")
     if os.path.exists(old):
         prev = np.load(old)
         for k in prev.files:
-            if k.startswith(("cfg2_", "cfg3_", "cfg5_")) and k not in out:
+            if k.startswith(("cfg2_", "cfg3_", "cfg5_", "mtx_")) and k not in out:
                 out[k] = prev[k]
 
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)

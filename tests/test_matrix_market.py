@@ -100,3 +100,19 @@ def test_solve_matrix_read_from_file(M, ctx, restate, tmp_path):
     st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=1000)
     ref = restate.solve("cg", "ic0", (n0, rp, ci, v), b, rtol=1e-10, max_iter=1000)
     assert st == M.OK and abs(res.iterations - ref["iterations"]) <= 2
+
+
+def test_reference_fixtures_match_golden(golden):
+    # the arrays stored in tests/golden are what the reader gives on the
+    # reference's own fixture files (checked where the MTL4 tree is present)
+    root = os.environ.get("REFERENCE_ROOT", "")
+    d = os.path.join(root, "libs", "numeric", "mtl", "test", "matrix_market")
+    if not root or not os.path.isdir(d):
+        pytest.skip("REFERENCE_ROOT does not name the MTL4 tree here")
+    for name in ("bcsstk01", "bcspwr02", "jgl009", "plskz362", "dense_read"):
+        rc, A = read(os.path.join(d, name + ".mtx"))
+        assert rc == 0, name
+        k = "mtx_" + name
+        assert np.array_equal(A["starts"], golden[k + "_rp"]), name
+        assert np.array_equal(A["indices"], golden[k + "_ci"]), name
+        assert np.array_equal(np.array(A["data"]), golden[k + "_v"]), name
