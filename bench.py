@@ -604,14 +604,39 @@ def main():
 
     peak, peak_kind = peaks()
 
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
+
+    def cold_ms(fn, reps_):
+        """Mean ms of fn with the 126 MB L2 flushed (256 MB written) before
+        every launch; each launch bracketed by its own CUDA events on the
+        library's stream."""
+        evs = []
+        ctx.synchronize()
+        with torch.cuda.stream(stream):
+            for _ in range(reps_):
+                flush.zero_()
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                evs.append((e0, e1))
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / reps_
+
     def spmv_stats(dA_, n_, nnz_, reps_=100):
         dxs, dys = ctx.to_device(M.uniform(n_, 5)), ctx.array(n_)
         for _ in range(5):
             dA_.spmv(dxs, dys)
         ms, _ = timed(lambda: dA_.spmv(dxs, dys), reps_)
+        ms_cold = cold_ms(lambda: dA_.spmv(dxs, dys), 30)
         byt = nnz_ * 12 + 4 * (n_ + 1) + 2 * n_ * 8
         return {"ms": ms, "GBps": byt / ms / 1e6, "hbm_frac": byt / ms / 1e6 / peak,
-                "bytes": byt, "peak_kind": peak_kind}
+                "bytes": byt, "peak_kind": peak_kind,
+                "back_to_back": "mean of %d products back to back" % reps_,
+                "cold": {"ms": ms_cold, "GBps": byt / ms_cold / 1e6,
+                         "hbm_frac": byt / ms_cold / 1e6 / peak,
+                         "how": "L2 flushed before each product, per-launch CUDA events"}}
 
     spmv = spmv_stats(dA, n, nnz)
 
@@ -628,6 +653,7 @@ def main():
         P32.apply_f32(r32, z32)
     ms_apply32, _ = timed(lambda: P32.apply_f32(r32, z32), 50)
     ms_pass = ms_apply32 / (2 * JACOBI_K)
+    ms_pass_cold = cold_ms(lambda: P32.apply_f32(r32, z32), 30) / (2 * JACOBI_K)
     x32 = ctx.to_device(M.uniform(n, 5).astype(np.float32))
     y32 = ctx.array(n, np.float32)
     for _ in range(5):
@@ -701,7 +727,9 @@ def main():
                      "ms": d_ms, "peak_kind": peak_kind},
         "mixed_kernels": {"jacobi_pass_f32": {"ms": ms_pass, "GBps": bytes_pass / ms_pass / 1e6,
                                               "bytes": bytes_pass,
-                                              "launches_per_iteration": 2 * JACOBI_K},
+                                              "launches_per_iteration": 2 * JACOBI_K,
+                                              "cold_ms": ms_pass_cold,
+                                              "cold_GBps": bytes_pass / ms_pass_cold / 1e6},
                           "spmv_f32": {"ms": ms_spmv32, "GBps": bytes_spmv32 / ms_spmv32 / 1e6,
                                        "bytes": bytes_spmv32}},
         "sweep_fp64": {"ms": ms_sweep64, "GBps": bytes_sweep64 / ms_sweep64 / 1e6,
