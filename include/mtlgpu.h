@@ -180,6 +180,44 @@ mtlgpu_status mtlgpu_csr_device_arrays(const mtlgpu_csr* A, const int32_t** d_ro
 /* A^T as a new handle (rows sorted by column), for adjoint solves of an
  * unsymmetric A (trans(A), transposed_sparse_matrix_vector_product_test.cpp:32). */
 mtlgpu_status mtlgpu_csr_create_transpose(mtlgpu_csr* A, mtlgpu_csr** out);
+
+/* ---- assembly --------------------------------------------------------------
+ * The updaters of mtl::mat::inserter (mtl/operation/update.hpp:26-111): how a
+ * value inserted at (r, c) combines with the entry already there, and what a
+ * new entry starts as (MINUS starts at -v, the others at v). */
+typedef enum {
+  MTLGPU_UPDATE_STORE = 0,  /* x = v   (ins[r][c] << v with the default updater, ins[r][c] = v) */
+  MTLGPU_UPDATE_PLUS = 1,   /* x += v  (ins[r][c] += v; inserter<M, update_plus<T>>)           */
+  MTLGPU_UPDATE_MINUS = 2,  /* x -= v  (inserter<M, update_minus<T>>)                           */
+  MTLGPU_UPDATE_TIMES = 3   /* x *= v  (inserter<M, update_times<T>>)                           */
+} mtlgpu_updater;
+
+/* Assembly from coordinate triplets on the device: the matrix that
+ *   { mtl::mat::inserter<compressed2D<double>, Updater> ins(A);
+ *     for k in 0..count-1: ins[d_rows[k]][d_cols[k]] << d_vals[k]; }
+ * leaves (mtl/matrix/compressed2D.hpp:662-1151; modify() 947-989).  Triplets
+ * apply in order, duplicates fold in that order, and the rows come out sorted
+ * without duplicates, bit-identical to the reference's inserter.
+ *   base     NULL: A starts empty; else A starts as a copy of base (the
+ *            inserter on a matrix that holds entries, stretch() 864-914);
+ *            n_rows / n_cols must then equal base's.
+ *   d_ops    NULL: `updater` for every triplet; else a device array of count
+ *            mtlgpu_updater bytes, one per triplet (ins[r][c] = v is STORE,
+ *            ins[r][c] += v is PLUS whatever the inserter's updater).
+ * Indices outside the matrix give MTLGPU_INDEX_RANGE (the reference's "Index
+ * is out of range!").  All arrays are device arrays; *out is a new handle. */
+mtlgpu_status mtlgpu_csr_assemble(mtlgpu_ctx* ctx, const mtlgpu_csr* base, int n_rows, int n_cols,
+                                  long long count, const int32_t* d_rows, const int32_t* d_cols,
+                                  const double* d_vals, const uint8_t* d_ops, int updater,
+                                  mtlgpu_csr** out);
+/* laplacian_setup(A, m, n) (mtl/matrix/laplacian_setup.hpp:25-44) built on
+ * the device: the m*n x m*n 5-point Laplacian (4 on the diagonal, -1 to each
+ * grid neighbour), identical to the reference's. */
+mtlgpu_status mtlgpu_csr_laplacian2d(mtlgpu_ctx* ctx, int m, int n, mtlgpu_csr** out);
+/* The 3-D 7-point Laplacian on an N^3 grid (row (i*N+j)*N+k, 6 on the
+ * diagonal, -1 to each neighbour inside the grid), built on the device; the
+ * reference has no 3-D setup, this is the 3-D counterpart of laplacian_setup. */
+mtlgpu_status mtlgpu_csr_laplacian3d(mtlgpu_ctx* ctx, int N, mtlgpu_csr** out);
 /* Gradient of a loss with respect to A's stored values in the solve
  * x = A^{-1} b, given the adjoint d_lambda (A^T lambda = dL/dx):
  * d_grad[k] = -lambda[i] * x[j] for the k-th stored entry (i, j).  The

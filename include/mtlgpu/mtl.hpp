@@ -548,6 +548,45 @@ class compressed2D {
     create(n, m, nnz, s.data(), ix.data(), nnz ? A.address_data() : nullptr);
   }
 #endif
+  /// An empty num_rows x num_cols matrix (compressed2D(r, c), filled by an
+  /// inserter or laplacian_setup).
+  compressed2D(int num_rows, int num_cols, context& c = context::default_context()) : ctx_(c) {
+    change_dim(num_rows, num_cols);
+  }
+  /// change_dim (compressed2D.hpp:441-451): new dimensions, no entries.
+  void change_dim(int num_rows, int num_cols) {
+    std::vector<int32_t> s(size_t(num_rows) + 1, 0);
+    create(num_rows, num_cols, 0, s.data(), nullptr, nullptr);
+  }
+  /// Take ownership of a handle built by the library (assembly, generators).
+  void adopt(mtlgpu_csr* A) {
+    int n = 0, m = 0, nz = 0;
+    throw_on(mtlgpu_csr_info(A, &n, &m, &nz), ctx_.get());
+    h_.reset(A, [](mtlgpu_csr* p) { mtlgpu_csr_destroy(p); });
+    n_rows_ = n;
+    n_cols_ = m;
+    nnz_ = nz;
+  }
+  /// The CSR arrays copied to the host.
+  host_csr to_host() const {
+    host_csr h;
+    h.num_rows = n_rows_;
+    h.num_cols = n_cols_;
+    h.starts.resize(size_t(n_rows_) + 1);
+    h.indices.resize(size_t(nnz_));
+    h.data.resize(size_t(nnz_));
+    const int32_t *rp = nullptr, *ci = nullptr;
+    const double* v = nullptr;
+    throw_on(mtlgpu_csr_device_arrays(handle(), &rp, &ci, &v), ctx_.get());
+    throw_on(mtlgpu_memcpy_d2h(ctx_.get(), h.starts.data(), rp, sizeof(int32_t) * h.starts.size()),
+             ctx_.get());
+    if (nnz_) {
+      throw_on(mtlgpu_memcpy_d2h(ctx_.get(), h.indices.data(), ci, sizeof(int32_t) * nnz_),
+               ctx_.get());
+      throw_on(mtlgpu_memcpy_d2h(ctx_.get(), h.data.data(), v, sizeof(double) * nnz_), ctx_.get());
+    }
+    return h;
+  }
   int num_rows() const { return n_rows_; }
   int num_cols() const { return n_cols_; }
   int nnz() const { return nnz_; }
@@ -590,6 +629,110 @@ template <typename Value>
 inline mat_cvec_product<Value> operator*(const compressed2D<Value>& A, const dense_vector<Value>& x) {
   return {&A, &x};
 }
+/// Updater code of the C ABI for an updater type (mtl/operation/update.hpp:26-111).
+template <typename Updater>
+struct updater_code {
+  static const int value = MTLGPU_UPDATE_STORE;
+};
+
+/// Insertion into a device matrix with the semantics of
+/// mtl::mat::inserter<compressed2D, Updater> (mtl/matrix/compressed2D.hpp:
+/// 662-1151): ins[r][c] << v applies the inserter's updater, ins[r][c] = v
+/// stores, ins[r][c] += v adds; entries the matrix already holds are kept
+/// and updated.  Triplets are collected on the host and assembled on the
+/// device (mtlgpu_csr_assemble) by finish() or the destructor, as the
+/// reference's inserter finishes in its destructor.  The slot size is
+/// accepted for interface compatibility; it never changes the result.
+template <typename Updater>
+class device_inserter {
+ public:
+  typedef double value_type;
+  explicit device_inserter(compressed2D<double>& A, int slot_size = 5) : A_(A) {
+    (void)slot_size;
+  }
+  device_inserter(const device_inserter&) = delete;
+  device_inserter& operator=(const device_inserter&) = delete;
+  ~device_inserter() {
+    try {
+      finish();
+    } catch (...) {  // a destructor must not throw; call finish() to see errors
+    }
+  }
+  struct proxy {
+    device_inserter& ins;
+    int r, c;
+    template <typename V>
+    proxy& operator<<(const V& v) {
+      ins.add(r, c, double(v), updater_code<Updater>::value);
+      return *this;
+    }
+    template <typename V>
+    proxy& operator=(const V& v) {
+      ins.add(r, c, double(v), MTLGPU_UPDATE_STORE);
+      return *this;
+    }
+    template <typename V>
+    proxy& operator+=(const V& v) {
+      ins.add(r, c, double(v), MTLGPU_UPDATE_PLUS);
+      return *this;
+    }
+  };
+  struct bracket {
+    device_inserter& ins;
+    int r;
+    proxy operator[](int c) { return {ins, r, c}; }
+  };
+  bracket operator[](int r) { return {*this, r}; }
+  proxy operator()(int r, int c) { return {*this, r, c}; }
+
+  /// Assembles the collected triplets into the matrix (once).
+  void finish() {
+    if (done_) return;
+    done_ = true;
+    mtlgpu_ctx* ctx = A_.ctx().get();
+    const long long n = (long long)rows_.size();
+    void *dr = nullptr, *dc = nullptr, *dv = nullptr, *dop = nullptr;
+    auto release = [&]() {
+      for (void* p : {dr, dc, dv, dop})
+        if (p) mtlgpu_free(ctx, p);
+    };
+    mtlgpu_csr* out = nullptr;
+    int st = MTLGPU_OK;
+    if (n > 0) {
+      st = mtlgpu_malloc(ctx, sizeof(int32_t) * n, &dr);
+      if (st == MTLGPU_OK) st = mtlgpu_malloc(ctx, sizeof(int32_t) * n, &dc);
+      if (st == MTLGPU_OK) st = mtlgpu_malloc(ctx, sizeof(double) * n, &dv);
+      if (st == MTLGPU_OK) st = mtlgpu_malloc(ctx, n, &dop);
+      if (st == MTLGPU_OK) st = mtlgpu_memcpy_h2d(ctx, dr, rows_.data(), sizeof(int32_t) * n);
+      if (st == MTLGPU_OK) st = mtlgpu_memcpy_h2d(ctx, dc, cols_.data(), sizeof(int32_t) * n);
+      if (st == MTLGPU_OK) st = mtlgpu_memcpy_h2d(ctx, dv, vals_.data(), sizeof(double) * n);
+      if (st == MTLGPU_OK) st = mtlgpu_memcpy_h2d(ctx, dop, ops_.data(), n);
+    }
+    if (st == MTLGPU_OK)
+      st = mtlgpu_csr_assemble(ctx, A_.nnz() ? A_.handle() : nullptr, A_.num_rows(),
+                               A_.num_cols(), n, static_cast<const int32_t*>(dr),
+                               static_cast<const int32_t*>(dc), static_cast<const double*>(dv),
+                               static_cast<const uint8_t*>(dop), updater_code<Updater>::value,
+                               &out);
+    release();
+    throw_on(st, ctx);
+    A_.adopt(out);
+  }
+
+ private:
+  void add(int r, int c, double v, int op) {
+    rows_.push_back(r);
+    cols_.push_back(c);
+    vals_.push_back(v);
+    ops_.push_back(uint8_t(op));
+  }
+  compressed2D<double>& A_;
+  std::vector<int32_t> rows_, cols_;
+  std::vector<double> vals_;
+  std::vector<uint8_t> ops_;
+  bool done_ = false;
+};
+
 template <typename Value>
 struct transposed_view {
   const compressed2D<Value>* A;
@@ -839,6 +982,78 @@ int solve(int method, const compressed2D<double>& A, dense_vector<double>& x,
 
 }  // namespace detail
 }  // namespace gpu
+
+#ifndef MTLGPU_WITH_MTL4
+// The updaters of mtl/operation/update.hpp:26-111 (standalone definitions).
+namespace operations {
+template <typename Element>
+struct update_store {
+  template <typename Value>
+  Element& operator()(Element& x, const Value& y) { return x = Element(y); }
+  template <typename Value>
+  Element init(const Value& y) { return y; }
+};
+template <typename Element>
+struct update_plus {
+  template <typename Value>
+  Element& operator()(Element& x, const Value& y) { return x += Element(y); }
+  template <typename Value>
+  Element init(const Value& y) { return y; }
+};
+template <typename Element>
+struct update_minus {
+  template <typename Value>
+  Element& operator()(Element& x, const Value& y) { return x -= Element(y); }
+  template <typename Value>
+  Element init(const Value& y) { return -y; }
+};
+template <typename Element>
+struct update_times {
+  template <typename Value>
+  Element& operator()(Element& x, const Value& y) { return x *= y; }
+  template <typename Value>
+  Element init(const Value& y) { return y; }
+};
+}  // namespace operations
+namespace mat {
+/// mtl::mat::inserter (mtl/matrix/inserter.hpp:33-52), for device matrices.
+template <typename Matrix, typename Updater = operations::update_store<double>>
+struct inserter;
+}  // namespace mat
+#endif
+
+namespace gpu {
+template <>
+struct updater_code<mtl::operations::update_plus<double>> {
+  static const int value = MTLGPU_UPDATE_PLUS;
+};
+template <>
+struct updater_code<mtl::operations::update_minus<double>> {
+  static const int value = MTLGPU_UPDATE_MINUS;
+};
+template <>
+struct updater_code<mtl::operations::update_times<double>> {
+  static const int value = MTLGPU_UPDATE_TIMES;
+};
+}  // namespace gpu
+
+namespace mat {
+/// mtl::mat::inserter<gpu::compressed2D<double>, Updater>: the reference's
+/// inserter interface, assembled on the device (gpu::device_inserter).
+template <typename Updater>
+struct inserter<gpu::compressed2D<double>, Updater> : gpu::device_inserter<Updater> {
+  explicit inserter(gpu::compressed2D<double>& A, int slot_size = 5)
+      : gpu::device_inserter<Updater>(A, slot_size) {}
+};
+
+/// laplacian_setup(A, m, n) (mtl/matrix/laplacian_setup.hpp:25-44) on a
+/// device matrix: the m*n x m*n 5-point Laplacian generated on the device.
+inline void laplacian_setup(gpu::compressed2D<double>& A, unsigned m, unsigned n) {
+  mtlgpu_csr* out = nullptr;
+  gpu::throw_on(mtlgpu_csr_laplacian2d(A.ctx().get(), int(m), int(n), &out), A.ctx().get());
+  A.adopt(out);
+}
+}  // namespace mat
 
 #ifdef MTLGPU_WITH_MTL4
 template <typename V>

@@ -99,6 +99,41 @@ void csr_release(Csr* A) {
 }
 
 }  // namespace
+
+// A new handle that takes ownership of device CSR arrays built by the library
+// (assembly, generators); they are freed with the handle, or here on failure.
+mtlgpu_status csr_adopt(Ctx* ctx, int n_rows, int n_cols, int nnz, int32_t* d_rp, int32_t* d_ci,
+                        double* d_v, Csr** out) {
+  *out = nullptr;
+  mtlgpu_csr* A = new (std::nothrow) mtlgpu_csr();
+  if (!A) {
+    dfree(ctx, d_rp);
+    dfree(ctx, d_ci);
+    dfree(ctx, d_v);
+    return MTLGPU_OUT_OF_MEMORY;
+  }
+  A->ctx = ctx;
+  A->n_rows = n_rows;
+  A->n_cols = n_cols;
+  A->nnz = nnz;
+  A->d_rp = d_rp;
+  A->d_ci = d_ci;
+  A->d_v = d_v;
+  mtlgpu_status s = csr_finish_create(A);
+  if (s != MTLGPU_OK) {
+    csr_release(A);
+    delete A;
+    return s;
+  }
+  *out = A;
+  return MTLGPU_OK;
+}
+
+mtlgpu_status csr_assemble(Ctx* ctx, const Csr* base, int n_rows, int n_cols, long long count,
+                           const int32_t* d_rows, const int32_t* d_cols, const double* d_vals,
+                           const uint8_t* d_ops, int updater, Csr** out);  // assemble.cu
+mtlgpu_status csr_laplacian(Ctx* ctx, int dim, int a, int b, Csr** out);   // assemble.cu
+
 }  // namespace mtlgpu
 
 using namespace mtlgpu;
@@ -309,6 +344,45 @@ mtlgpu_status mtlgpu_csr_destroy(mtlgpu_csr* A) {
   csr_release(A);
   cudaStreamSynchronize(c->stream);
   delete A;
+  return MTLGPU_OK;
+}
+
+mtlgpu_status mtlgpu_csr_assemble(mtlgpu_ctx* c, const mtlgpu_csr* base, int n_rows, int n_cols,
+                                  long long count, const int32_t* d_rows, const int32_t* d_cols,
+                                  const double* d_vals, const uint8_t* d_ops, int updater,
+                                  mtlgpu_csr** out) {
+  if (!c || !out || n_rows < 0 || n_cols < 0 || count < 0 ||
+      (count > 0 && (!d_rows || !d_cols || !d_vals)) || updater < MTLGPU_UPDATE_STORE ||
+      updater > MTLGPU_UPDATE_TIMES)
+    return MTLGPU_INVALID_ARG;
+  if (base && (base->ctx != c || base->n_rows != n_rows || base->n_cols != n_cols))
+    return MTLGPU_INCOMPATIBLE_SIZE;
+  *out = nullptr;
+  MTLGPU_TRY(set_device(c));
+  Csr* A = nullptr;
+  MTLGPU_TRY(csr_assemble(c, base, n_rows, n_cols, count, d_rows, d_cols, d_vals, d_ops, updater,
+                          &A));
+  *out = static_cast<mtlgpu_csr*>(A);
+  return MTLGPU_OK;
+}
+
+mtlgpu_status mtlgpu_csr_laplacian2d(mtlgpu_ctx* c, int m, int n, mtlgpu_csr** out) {
+  if (!c || !out || m < 0 || n < 0) return MTLGPU_INVALID_ARG;
+  *out = nullptr;
+  MTLGPU_TRY(set_device(c));
+  Csr* A = nullptr;
+  MTLGPU_TRY(csr_laplacian(c, 2, m, n, &A));
+  *out = static_cast<mtlgpu_csr*>(A);
+  return MTLGPU_OK;
+}
+
+mtlgpu_status mtlgpu_csr_laplacian3d(mtlgpu_ctx* c, int N, mtlgpu_csr** out) {
+  if (!c || !out || N < 0) return MTLGPU_INVALID_ARG;
+  *out = nullptr;
+  MTLGPU_TRY(set_device(c));
+  Csr* A = nullptr;
+  MTLGPU_TRY(csr_laplacian(c, 3, N, N, &A));
+  *out = static_cast<mtlgpu_csr*>(A);
   return MTLGPU_OK;
 }
 

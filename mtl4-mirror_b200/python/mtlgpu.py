@@ -30,6 +30,7 @@ CG, BICGSTAB = 0, 1
 METHODS = {"cg": CG, "bicgstab": BICGSTAB}
 SOLVE_FP64, SOLVE_MIXED = 0, 1
 LOWER, UPPER = 0, 1
+UPDATE_STORE, UPDATE_PLUS, UPDATE_MINUS, UPDATE_TIMES = range(4)
 
 _vp = C.c_void_p
 
@@ -79,6 +80,10 @@ def _lib():
         L.mtlgpu_dot.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(C.c_double)]
         L.mtlgpu_two_norm.argtypes = [_vp, C.c_int, _vp, C.POINTER(C.c_double)]
         L.mtlgpu_unary_dot.argtypes = [_vp, C.c_int, _vp, C.POINTER(C.c_double)]
+        L.mtlgpu_csr_assemble.argtypes = [_vp, _vp, C.c_int, C.c_int, C.c_longlong, _vp, _vp,
+                                          _vp, _vp, C.c_int, C.POINTER(_vp)]
+        L.mtlgpu_csr_laplacian2d.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(_vp)]
+        L.mtlgpu_csr_laplacian3d.argtypes = [_vp, C.c_int, C.POINTER(_vp)]
         _LIB = L
     return _LIB
 
@@ -240,6 +245,69 @@ class Csr:
         st = _lib().mtlgpu_csr_create(ctx.h, self.n, self.n_cols, self.nnz, _p(rp), _p(ci), _p(v),
                                       C.byref(self.h))
         check(st, "csr_create")
+
+    @classmethod
+    def _adopt(cls, ctx, h):
+        A = cls.__new__(cls)
+        A.ctx, A.h = ctx, h
+        n, m, nnz = C.c_int(), C.c_int(), C.c_int()
+        check(_lib().mtlgpu_csr_info(h, C.byref(n), C.byref(m), C.byref(nnz)), "csr_info")
+        A.n, A.n_cols, A.nnz = n.value, m.value, nnz.value
+        return A
+
+    @classmethod
+    def assemble(cls, ctx, n_rows, n_cols, rows, cols, vals, ops=None, updater=UPDATE_STORE,
+                 base=None):
+        """mtl::mat::inserter on the device (mtlgpu_csr_assemble): triplets
+        (device arrays, or numpy arrays uploaded here) inserted in order into
+        an empty n_rows x n_cols matrix, or into a copy of `base`."""
+        keep = []
+
+        def dev(a, dt):
+            if a is None or isinstance(a, DeviceArray):
+                return a
+            d = ctx.to_device(np.ascontiguousarray(a, dt))
+            keep.append(d)
+            return d
+        r, c, v, o = dev(rows, np.int32), dev(cols, np.int32), dev(vals, np.float64), \
+            dev(ops, np.uint8)
+        count = r.n if r is not None else 0
+        h = _vp()
+        check(_lib().mtlgpu_csr_assemble(ctx.h, base.h if base is not None else None, n_rows,
+                                         n_cols, count, r.ptr if count else None,
+                                         c.ptr if count else None, v.ptr if count else None,
+                                         o.ptr if o is not None else None, int(updater),
+                                         C.byref(h)), "csr_assemble")
+        return cls._adopt(ctx, h)
+
+    @classmethod
+    def laplacian2d(cls, ctx, m, n):
+        """laplacian_setup(A, m, n) built on the device."""
+        h = _vp()
+        check(_lib().mtlgpu_csr_laplacian2d(ctx.h, m, n, C.byref(h)), "csr_laplacian2d")
+        return cls._adopt(ctx, h)
+
+    @classmethod
+    def laplacian3d(cls, ctx, N):
+        """The 3-D 7-point Laplacian on an N^3 grid built on the device."""
+        h = _vp()
+        check(_lib().mtlgpu_csr_laplacian3d(ctx.h, N, C.byref(h)), "csr_laplacian3d")
+        return cls._adopt(ctx, h)
+
+    def download(self):
+        """(rp, ci, v) host copies of the CSR arrays."""
+        rp_, ci_, v_ = _vp(), _vp(), _vp()
+        check(_lib().mtlgpu_csr_device_arrays(self.h, C.byref(rp_), C.byref(ci_), C.byref(v_)),
+              "csr_device_arrays")
+        rp = np.empty(self.n + 1, np.int32)
+        ci = np.empty(self.nnz, np.int32)
+        v = np.empty(self.nnz, np.float64)
+        L = _lib()
+        check(L.mtlgpu_memcpy_d2h(self.ctx.h, _p(rp), rp_, rp.nbytes), "d2h")
+        if self.nnz:
+            check(L.mtlgpu_memcpy_d2h(self.ctx.h, _p(ci), ci_, ci.nbytes), "d2h")
+            check(L.mtlgpu_memcpy_d2h(self.ctx.h, _p(v), v_, v.nbytes), "d2h")
+        return rp, ci, v
 
     def set_values(self, v):
         v = np.ascontiguousarray(v, np.float64)

@@ -51,6 +51,7 @@ class _Base:
         getattr(L, p + "solve").restype = C.c_int
         getattr(L, p + "pc_apply").restype = C.c_int
         getattr(L, p + "laplacian_setup").restype = C.c_int
+        getattr(L, p + "assemble").restype = C.c_int
 
     def _f(self, name):
         return getattr(self.lib, self.prefix + name)
@@ -64,6 +65,49 @@ class _Base:
         v = np.zeros(nnz, np.float64)
         f(C.c_uint(m), C.c_uint(n), _ptr(rp), _ptr(ci), _ptr(v))
         return (m * n, rp, ci, v)
+
+    def assemble(self, n_rows, n_cols, rows, cols, vals, ops=None, updater=0, base=None,
+                 syntax=None, slot_size=0):
+        """The matrix mtl::mat::inserter leaves after the triplets (see
+        or_assemble / ref_assemble): returns (rp, ci, v), or raises
+        IndexError for an index out of range.  The restatement takes `ops`
+        (updater per triplet); the reference takes `syntax` (0: ins = v,
+        1: ins += v, 2: ins << v with the class updater)."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        if base is not None:
+            brp, bci, bv = (np.ascontiguousarray(base[0], np.int32),
+                            np.ascontiguousarray(base[1], np.int32),
+                            np.ascontiguousarray(base[2], np.float64))
+            bn = len(bci)
+        else:
+            brp = bci = bv = None
+            bn = 0
+        cap = max(1, bn + len(rows))
+        rp = np.zeros(n_rows + 1, np.int32)
+        ci = np.zeros(cap, np.int32)
+        v = np.zeros(cap, np.float64)
+        if self.prefix == "ref_":
+            sx = None if syntax is None else np.ascontiguousarray(syntax, np.uint8)
+            secs = C.c_double()
+            nnz = self._f("assemble")(C.c_int(n_rows), C.c_int(n_cols), C.c_int(bn), _ptr(brp),
+                                      _ptr(bci), _ptr(bv), C.c_longlong(len(rows)), _ptr(rows),
+                                      _ptr(cols), _ptr(vals), _ptr(sx), C.c_int(updater),
+                                      C.c_int(slot_size), _ptr(rp), _ptr(ci), _ptr(v),
+                                      C.byref(secs))
+            self.last_seconds = secs.value
+        else:
+            o = None if ops is None else np.ascontiguousarray(ops, np.uint8)
+            nnz = self._f("assemble")(C.c_int(n_rows), C.c_int(n_cols), C.c_int(bn), _ptr(brp),
+                                      _ptr(bci), _ptr(bv), C.c_longlong(len(rows)), _ptr(rows),
+                                      _ptr(cols), _ptr(vals), _ptr(o), C.c_int(updater),
+                                      _ptr(rp), _ptr(ci), _ptr(v))
+        if nnz == -1:
+            raise IndexError("Index is out of range!")
+        if nnz < 0:
+            raise RuntimeError(f"assemble failed ({nnz})")
+        return rp, ci[:nnz].copy(), v[:nnz].copy()
 
     def spmv(self, A, x, y=None, mode=0):
         n, rp, ci, v = A

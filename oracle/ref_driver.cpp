@@ -309,6 +309,57 @@ int ref_solve(int method, int pc, int n, int nnz, const int* rp, const int* ci, 
   return err;
 }
 
+// Assembly through mtl::mat::inserter<compressed2D, Updater>
+// (compressed2D.hpp:662-1151, update.hpp:26-111).  The matrix starts as the
+// base CSR (base_nnz entries, possibly none); then every triplet k goes in as
+// ins[rows[k]][cols[k]] << vals[k] (the class updater: 0 store, 1 plus,
+// 2 minus, 3 times), or, with syntax != nullptr, as syntax[k] == 0:
+// ins[r][c] = v, 1: ins[r][c] += v, 2: ins[r][c] << v.  slot_size is the
+// inserter's (5 when 0).  The result is exported to rp / ci / v (capacity
+// base_nnz + count entries); returns nnz, -1 on an updater out of range.
+// *seconds receives the time from the inserter's construction to its
+// destruction.
+int ref_assemble(int n_rows, int n_cols, int base_nnz, const int* brp, const int* bci,
+                 const double* bv, long long count, const int* rows, const int* cols,
+                 const double* vals, const unsigned char* syntax, int updater, int slot_size,
+                 int* rp, int* ci, double* v, double* seconds) {
+  const unsigned nr = unsigned(n_rows), nc = unsigned(n_cols);
+  matrix_type A(nr, nc);
+  if (base_nnz > 0) {
+    std::vector<unsigned> major(brp, brp + n_rows + 1), minor(bci, bci + base_nnz);
+    std::vector<double> data(bv, bv + base_nnz);
+    matrix_type B(nr, nc, unsigned(base_nnz), major.data(),
+                  minor.data(), data.data());
+    A = B;
+  }
+  const unsigned slots = slot_size > 0 ? unsigned(slot_size) : 5u;
+  auto run = [&](auto updater_tag) {
+    typedef decltype(updater_tag) U;
+    auto t0 = std::chrono::steady_clock::now();
+    {
+      mtl::mat::inserter<matrix_type, U> ins(A, slots);
+      for (long long k = 0; k < count; ++k) {
+        const unsigned r = unsigned(rows[k]), c = unsigned(cols[k]);
+        if (!syntax || syntax[k] == 2)
+          ins[r][c] << vals[k];
+        else if (syntax[k] == 0)
+          ins[r][c] = vals[k];
+        else
+          ins[r][c] += vals[k];
+      }
+    }
+    if (seconds) *seconds = seconds_since(t0);
+  };
+  switch (updater) {
+    case 0: run(mtl::operations::update_store<double>()); break;
+    case 1: run(mtl::operations::update_plus<double>()); break;
+    case 2: run(mtl::operations::update_minus<double>()); break;
+    case 3: run(mtl::operations::update_times<double>()); break;
+    default: return -1;
+  }
+  return export_csr(A, rp, ci, v);
+}
+
 // Build-flavour tag, so callers can report how the baseline was compiled.
 const char* ref_build_info(void) {
 #ifdef MTL_WITH_OPENMP

@@ -584,3 +584,81 @@ int or_solve(int method, int pc, int n, const int* rp, const int* ci, const doub
   pc_free(&P);
   return err;
 }
+
+/* Assembly through mtl::mat::inserter<compressed2D, Updater>
+ * (mtl/matrix/compressed2D.hpp:662-1151).  Each row is kept as a sorted
+ * (column, value) list, the union of the inserter's slot and spare map.
+ * modify() (947-989) looks the entry up: present -> the updater of
+ * update.hpp:26-111 (0 store x = y, 1 plus x += y, 2 minus x -= y, 3 times
+ * x *= y); absent -> inserted with init(y) (minus: -y, else y).  The matrix
+ * starts as the base CSR (stretch(), 864-914, keeps its entries); triplet k
+ * uses ops[k] when ops != NULL, else `updater`.  Output: rp (n_rows+1), ci, v
+ * with room for base_nnz + count entries; returns nnz, or -1 for an index
+ * out of range (the reference's "Index is out of range!"). */
+typedef struct {
+  int n, cap;
+  int* c;
+  double* v;
+} or_row;
+
+int or_assemble(int n_rows, int n_cols, int base_nnz, const int* brp, const int* bci,
+                const double* bv, long long count, const int* rows, const int* cols,
+                const double* vals, const unsigned char* ops, int updater, int* rp, int* ci,
+                double* v) {
+  or_row* R = (or_row*)calloc(n_rows > 0 ? (size_t)n_rows : 1, sizeof(or_row));
+  int ret = 0;
+  if (!R) return -2;
+  for (int r = 0; r < n_rows && base_nnz > 0; r++) {
+    const int len = brp[r + 1] - brp[r];
+    R[r].cap = len > 4 ? len : 4;
+    R[r].c = (int*)malloc(sizeof(int) * (size_t)R[r].cap);
+    R[r].v = (double*)malloc(sizeof(double) * (size_t)R[r].cap);
+    for (int j = 0; j < len; j++) R[r].c[j] = bci[brp[r] + j], R[r].v[j] = bv[brp[r] + j];
+    R[r].n = len;
+  }
+  for (long long k = 0; k < count; k++) {
+    const int r = rows[k], c = cols[k];
+    const int op = ops ? (int)ops[k] : updater;
+    if (r < 0 || r >= n_rows || c < 0 || c >= n_cols) {
+      ret = -1;
+      break;
+    }
+    or_row* w = &R[r];
+    int lo = 0, hi = w->n;            /* first position with column >= c */
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (w->c[mid] < c) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < w->n && w->c[lo] == c) {
+      double* x = &w->v[lo];
+      if (op == 1) *x = *x + vals[k];
+      else if (op == 2) *x = *x - vals[k];
+      else if (op == 3) *x = *x * vals[k];
+      else *x = vals[k];
+      continue;
+    }
+    if (w->n == w->cap) {
+      w->cap = w->cap ? 2 * w->cap : 4;
+      w->c = (int*)realloc(w->c, sizeof(int) * (size_t)w->cap);
+      w->v = (double*)realloc(w->v, sizeof(double) * (size_t)w->cap);
+    }
+    memmove(w->c + lo + 1, w->c + lo, sizeof(int) * (size_t)(w->n - lo));
+    memmove(w->v + lo + 1, w->v + lo, sizeof(double) * (size_t)(w->n - lo));
+    w->c[lo] = c;
+    w->v[lo] = op == 2 ? -vals[k] : vals[k];
+    w->n++;
+  }
+  if (ret == 0) {
+    int nnz = 0;
+    rp[0] = 0;
+    for (int r = 0; r < n_rows; r++) {
+      for (int j = 0; j < R[r].n; j++) ci[nnz] = R[r].c[j], v[nnz] = R[r].v[j], nnz++;
+      rp[r + 1] = nnz;
+    }
+    ret = nnz;
+  }
+  for (int r = 0; r < n_rows; r++) free(R[r].c), free(R[r].v);
+  free(R);
+  return ret;
+}

@@ -67,6 +67,14 @@ int or_solve(int method, int pc, int n, const int* rp, const int* ci, const doub
              const double* b, double* x, int max_iter, double rtol, double atol, double norm_r0,
              double* hist, int hist_cap, double* out);
 
+/* Assembly through mtl::mat::inserter (compressed2D.hpp:662-1151) from a base
+ * CSR plus coordinate triplets; ops[k] (or `updater` for all) is 0 store,
+ * 1 plus, 2 minus, 3 times.  Returns nnz, -1 on an index out of range. */
+int or_assemble(int n_rows, int n_cols, int base_nnz, const int* brp, const int* bci,
+                const double* bv, long long count, const int* rows, const int* cols,
+                const double* vals, const unsigned char* ops, int updater, int* rp, int* ci,
+                double* v);
+
 #ifdef __cplusplus
 }
 #endif

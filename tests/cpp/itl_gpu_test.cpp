@@ -299,6 +299,66 @@ void case_errors() {
 
 }  // namespace
 
+// laplacian_setup_test / the inserter (compressed2D.hpp:662-1151) on device
+// matrices: the 5-point Laplacian inserted element by element as
+// laplacian_setup.hpp:30-41 does equals the device laplacian_setup and the
+// host generator; duplicates fold with the inserter's updater; an index out
+// of range raises index_out_of_range.
+void case_assemble() {
+  const int m = 20, n = 30;
+  Matrix A(m * n, m * n), L(0, 0);
+  {
+    mtl::mat::inserter<Matrix> ins(A, 5);
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) {
+        const int row = i * n + j;
+        ins(row, row) << 4.0;
+        if (j < n - 1) ins(row, row + 1) << -1.0;
+        if (i < m - 1) ins(row, row + n) << -1.0;
+        if (j > 0) ins(row, row - 1) << -1.0;
+        if (i > 0) ins(row, row - n) << -1.0;
+      }
+  }
+  mtl::mat::laplacian_setup(L, m, n);
+  HostCsr h = laplacian2d(m, n);
+  const mtl::gpu::host_csr a = A.to_host(), l = L.to_host();
+  const bool lap_equal = a.starts == l.starts && a.indices == l.indices && a.data == l.data &&
+                         a.starts == h.rp && a.indices == h.ci && a.data == h.v;
+  // update_plus with duplicates, then `=` and `+=` on top of the result
+  Matrix B(3, 4);
+  {
+    mtl::mat::inserter<Matrix, mtl::operations::update_plus<double>> ins(B);
+    ins[2][3] << 1.5;
+    ins[0][1] << 2.0;
+    ins[2][3] << 0.25;
+    ins[1][0] << -1.0;
+  }
+  {
+    mtl::mat::inserter<Matrix> ins(B);
+    ins[2][3] += 4.0;   // 1.75 + 4
+    ins[0][1] = 7.0;    // overwritten
+    ins[0][0] << 3.0;   // new entry
+  }
+  const mtl::gpu::host_csr b = B.to_host();
+  const bool upd_ok = b.starts == std::vector<int32_t>{0, 2, 3, 4} &&
+                      b.indices == std::vector<int32_t>{0, 1, 0, 3} &&
+                      b.data == std::vector<double>{3.0, 7.0, -1.0, 5.75};
+  bool range_error = false;
+  try {
+    Matrix C(2, 2);
+    mtl::mat::inserter<Matrix> ins(C);
+    ins[0][2] << 1.0;
+    ins.finish();
+  } catch (const mtl::index_out_of_range&) {
+    range_error = true;
+  }
+  check(lap_equal && upd_ok && range_error, "device inserter");
+  std::printf("{\"case\": \"assemble\", \"laplacian_equal\": %s, \"updaters\": %s, "
+              "\"range_error\": %s, \"nnz\": %d}\n",
+              lap_equal ? "true" : "false", upd_ok ? "true" : "false",
+              range_error ? "true" : "false", A.nnz());
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) {
     std::fprintf(stderr, "usage: itl_gpu_test spmv|dot|ic0_float|cg|bicgstab|mixed|errors\n");
@@ -314,6 +374,7 @@ int main(int argc, char** argv) {
     else if (c == "mixed") case_mixed();
     else if (c == "errors") case_errors();
     else if (c == "adjoint") case_adjoint();
+    else if (c == "assemble") case_assemble();
     else {
       std::fprintf(stderr, "unknown case %s\n", c.c_str());
       return 2;

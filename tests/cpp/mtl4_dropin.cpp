@@ -151,6 +151,61 @@ void case_pc() {
               max_abs_diff(y, dy), max_abs_diff(yi, dyi), max_abs_diff(ya, dya));
 }
 
+// The same insertion code on mtl::compressed2D (the reference's inserter)
+// and on mtl::gpu::compressed2D (assembled on the device): seeded triplets
+// with duplicates, `<<` with update_plus, `=` and `+=` mixed, into a matrix
+// that already holds entries.  The CSR arrays must be identical.
+template <typename M>
+void insert_all(M& A, const std::vector<int>& r, const std::vector<int>& c,
+                const std::vector<double>& v, const std::vector<int>& how) {
+  mtl::mat::inserter<M, mtl::operations::update_plus<double>> ins(A, 3);
+  for (size_t k = 0; k < r.size(); ++k) {
+    if (how[k] == 0) ins[r[k]][c[k]] = v[k];
+    else if (how[k] == 1) ins[r[k]][c[k]] += v[k];
+    else ins[r[k]][c[k]] << v[k];
+  }
+}
+
+void case_assemble() {
+  const int nr = 400, nc = 300, cnt = 20000;
+  std::vector<int> r(cnt), c(cnt), how(cnt);
+  std::vector<double> v(cnt), u(cnt);
+  mtlgpu_gen_uniform(cnt, 91, -1.0, 1.0, v.data());
+  mtlgpu_gen_uniform(cnt, 92, 0.0, 1.0, u.data());
+  for (int k = 0; k < cnt; ++k) {
+    r[k] = int(u[k] * nr) % nr;
+    c[k] = (r[k] * 3 + k % 11) % nc;
+    how[k] = k % 3;
+  }
+  Matrix A(nr, nc);
+  insert_all(A, std::vector<int>(r.begin(), r.begin() + 5000),
+             std::vector<int>(c.begin(), c.begin() + 5000),
+             std::vector<double>(v.begin(), v.begin() + 5000), std::vector<int>(5000, 2));
+  insert_all(A, r, c, v, how);
+  DMatrix dA(nr, nc);
+  insert_all(dA, std::vector<int>(r.begin(), r.begin() + 5000),
+             std::vector<int>(c.begin(), c.begin() + 5000),
+             std::vector<double>(v.begin(), v.begin() + 5000), std::vector<int>(5000, 2));
+  insert_all(dA, r, c, v, how);
+  const mtl::gpu::host_csr h = dA.to_host();
+  bool same = int(A.nnz()) == dA.nnz();
+  for (int i = 0; same && i <= nr; ++i) same = int(A.ref_major()[i]) == h.starts[i];
+  for (int j = 0; same && j < dA.nnz(); ++j)
+    same = int(A.ref_minor()[j]) == h.indices[j] && A.data[j] == h.data[j];
+  // laplacian_setup on both matrix types
+  Matrix L(1, 1);
+  DMatrix dL(1, 1);
+  mtl::mat::laplacian_setup(L, 17, 23);
+  mtl::mat::laplacian_setup(dL, 17, 23);
+  const mtl::gpu::host_csr hl = dL.to_host();
+  bool lap = int(L.nnz()) == dL.nnz();
+  for (int j = 0; lap && j < dL.nnz(); ++j)
+    lap = int(L.ref_minor()[j]) == hl.indices[j] && L.data[j] == hl.data[j];
+  std::printf("{\"case\": \"assemble\", \"nnz\": %d, \"identical\": %s, "
+              "\"laplacian_identical\": %s}\n",
+              dA.nnz(), same ? "true" : "false", lap ? "true" : "false");
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -159,8 +214,9 @@ int main(int argc, char** argv) {
     if (c == "cg") case_cg();
     else if (c == "bicgstab") case_bicgstab();
     else if (c == "pc") case_pc();
+    else if (c == "assemble") case_assemble();
     else {
-      std::fprintf(stderr, "usage: mtl4_dropin cg|bicgstab|pc\n");
+      std::fprintf(stderr, "usage: mtl4_dropin cg|bicgstab|pc|assemble\n");
       return 2;
     }
   } catch (const std::exception& e) {

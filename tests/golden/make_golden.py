@@ -11,7 +11,8 @@ Run in a checkout where the reference tree is present (it is compiled by
                                                   # + the reference's Matrix Market fixtures
 
 Every array stored here is an output of the reference's own code path
-(laplacian_setup, compressed2D SpMV, ic_0 / ilu_0 factors, solve(P, x),
+(laplacian_setup, compressed2D SpMV, the compressed2D inserter, ic_0 /
+ilu_0 factors, solve(P, x),
 itl::cg / itl::bicgstab with basic_iteration), except the level arrays,
 which the reference does not compute: those come from the restatement
 (oracle/restate.c, or_levels_lower/upper) applied to the reference's own
@@ -129,6 +130,36 @@ def mtx_fixtures(R, S, out):
     out["mtx_bcsstk01_iters"] = np.array(its)
 
 
+def assembly_cases(R, out):
+    """mtl::mat::inserter runs of the reference on seeded triplets with many
+    duplicates (rows and columns drawn from small ranges), stored with their
+    inputs: 'asm_u<k>' inserts with `<<` and class updater k (store, plus,
+    minus, times) into an empty 300 x 250 matrix; 'asm_mix' mixes `=`, `+=`
+    and `<<` (class updater plus) on top of a base matrix with entries."""
+    rng = np.random.default_rng(7)
+    nr, nc, cnt = 300, 250, 6000
+    rows = rng.integers(0, nr, cnt).astype(np.int32)
+    cols = (rows.astype(np.int64) * 7 + rng.integers(0, 12, cnt)) % nc
+    cols = cols.astype(np.int32)
+    vals = rng.normal(size=cnt)
+    out["asm_rows"], out["asm_cols"], out["asm_vals"] = rows, cols, vals
+    out["asm_shape"] = np.array([nr, nc])
+    for u in range(4):
+        rp, ci, v = R.assemble(nr, nc, rows, cols, vals, updater=u)
+        out[f"asm_u{u}_rp"], out[f"asm_u{u}_ci"], out[f"asm_u{u}_v"] = rp, ci, v
+    # base matrix: 2 seeded entries per row (sorted, distinct columns)
+    brows = np.repeat(np.arange(nr, dtype=np.int32), 2)
+    bcols = np.sort(np.stack([rng.choice(nc, 2, replace=False) for _ in range(nr)]), axis=1)
+    bcols = bcols.ravel().astype(np.int32)
+    bvals = rng.normal(size=2 * nr)
+    base = R.assemble(nr, nc, brows, bcols, bvals)
+    out["asm_base_rp"], out["asm_base_ci"], out["asm_base_v"] = base
+    syntax = rng.integers(0, 3, cnt).astype(np.uint8)
+    out["asm_mix_syntax"] = syntax
+    rp, ci, v = R.assemble(nr, nc, rows, cols, vals, updater=1, base=base, syntax=syntax)
+    out["asm_mix_rp"], out["asm_mix_ci"], out["asm_mix_v"] = rp, ci, v
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
@@ -206,6 +237,8 @@ def main():
         rr = R.solve("cg", pc, A, b, rtol=1e-8, max_iter=1000)
         out[f"rg_{pc}_iters"] = np.array([rr["iterations"], rr["err"]])
         out[f"rg_{pc}_hist"] = rr["history"]
+
+    assembly_cases(R, out)
 
     # 2-D finite volume, 32^2 (seed 4)
     A = M.fv2d(32, 1.0, 8.0, 4)

@@ -146,3 +146,17 @@ def test_mtl4_dropin_preconditioners():
     r = _run("mtl4_dropin", "pc")
     assert r["ic0_float_max_diff"] <= 1e-12
     assert r["ilu0_max_diff"] <= 1e-14 and r["ilu0_adjoint_max_diff"] <= 1e-14
+
+
+@pytest.mark.gpu
+def test_device_inserter(built):
+    r = _run("itl_gpu_test", "assemble")
+    assert r["laplacian_equal"] and r["updaters"] and r["range_error"]
+    assert r["nnz"] == 5 * 600 - 2 * (20 + 30)
+
+
+@pytest.mark.gpu
+def test_mtl4_dropin_inserter():
+    _dropin()
+    r = _run("mtl4_dropin", "assemble")
+    assert r["identical"] and r["laplacian_identical"] and r["nnz"] > 0
