@@ -226,6 +226,14 @@ def cpu_baseline(M, A, b, A3, b3):
     # the reference's inserter on the same shuffled triplets (slot size 7, one
     # run): mtl::mat::inserter<compressed2D> from construction to destruction
     if kind == "reference":
+        # the other Krylov methods on the same 48^3 system as the device leg
+        Ak, bk = krylov_system(M)
+        kr = {}
+        for meth, pc, param, mx in KRYLOV_LEG:
+            rr = ref.solve_krylov(meth, pc, Ak, bk, param=param, max_iter=mx, rtol=1e-8)
+            kr[meth] = {"ms": 1e3 * rr["t_solve"], "iterations": rr["iterations"],
+                        "err": rr["err"]}
+        out["krylov_methods"] = kr
         _, r_, c_, v_ = assembly_triplets(M)
         ref.assemble(A[0], A[0], r_, c_, v_, slot_size=7)
         out["assembly_inserter_ms"] = 1e3 * ref.last_seconds
@@ -398,6 +406,48 @@ def assembly_workload(M, ctx, stream, peak):
             "ms": ms, "GBps_algorithmic": byt / ms / 1e6, "hbm_frac": byt / ms / 1e6 / peak,
             "identical_to_generator": identical, "includes": "sort, fold, row starts and the "
             "handle's SpMV layout analysis", "laplacian3d_generate_ms": ms_gen}
+
+
+KRYLOV_LEG = [("bicg", "identity", 0, 2000), ("cgs", "ilu0", 0, 2000),
+              ("bicgstab_2", "ilu0", 0, 2000), ("bicgstab_ell", "ilu0", 4, 2000),
+              ("tfqmr", "ilu0", 0, 2000), ("qmr", "ilu0", 0, 100), ("idr_s", "identity", 2, 4000),
+              ("gmres", "ilu0", 30, 300)]
+KRYLOV_GRID = 48
+
+
+def krylov_system(M):
+    A = M.convdiff27(KRYLOV_GRID, 2)
+    return A, M.csr_mult(A, M.uniform(A[0], 1))
+
+
+def krylov_workload(M, ctx, stream):
+    """The other Krylov methods (mtlgpu_solve_krylov, FP64, exact ILU(0)
+    triangular solves on the left where the method takes a preconditioner)
+    on the 27-point convection-diffusion operator 48^3 (n = 110,592), rtol
+    1e-8, x0 = 0: time per solve, iterations, true residual."""
+    A, b = krylov_system(M)
+    n = A[0]
+    dA = M.Csr(ctx, *A[1:])
+    P = M.Pc(dA, "ilu0")
+    db, dx, dz = ctx.to_device(b), ctx.array(n), ctx.to_device(np.zeros(n))
+    out = {"system": "27-point convection-diffusion %d^3, rtol 1e-8" % KRYLOV_GRID, "n": n}
+    for meth, pc, param, mx in KRYLOV_LEG:
+        L = P if pc == "ilu0" else None
+
+        def run():
+            ctx.xpay(dz, 0.0, dx)
+            st, res, _ = M.solve_krylov(meth, dA, L, dx, db, param=param, max_iter=mx,
+                                        rtol=1e-8)
+            return st, res
+        run()
+        ms, rr = _local_ms(run, 2, stream)
+        st, res = rr[-1]
+        out[meth] = {"ms": ms, "status": st, "iterations": res.iterations, "param": param,
+                     "pc_left": pc, "true_rel_residual": res.true_resid / np.linalg.norm(b),
+                     "kernel_launches": res.kernel_launches}
+    P.close()
+    dA.close()
+    return out
 
 
 def adjoint_workload(M, ctx, stream):
@@ -794,6 +844,7 @@ def main():
         line["batched"] = batched_workload(M, ctx, stream, peak)
         line["differentiable_solve"] = adjoint_workload(M, ctx, stream)
         line["assembly"] = assembly_workload(M, ctx, stream, peak)
+        line["krylov_methods"] = krylov_workload(M, ctx, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if A3 is None:
             A3 = M.convdiff27(CD_GRID, 2)

@@ -76,8 +76,21 @@ typedef enum {
   MTLGPU_PC_IC0 = 3
 } mtlgpu_pc_kind;
 
-/* itl/krylov/cg.hpp:75-112, itl/krylov/bicgstab.hpp:27-78 */
-typedef enum { MTLGPU_CG = 0, MTLGPU_BICGSTAB = 1 } mtlgpu_method;
+/* itl/krylov/cg.hpp:75-112, bicgstab.hpp:27-78, bicg.hpp:22-63, cgs.hpp:23-65,
+ * bicgstab_2.hpp:33-131, bicgstab_ell.hpp:37-132, tfqmr.hpp:26-100,
+ * qmr.hpp:24-109, idr_s.hpp:30-105, gmres.hpp:34-135 */
+typedef enum {
+  MTLGPU_CG = 0,
+  MTLGPU_BICGSTAB = 1,
+  MTLGPU_BICG = 2,
+  MTLGPU_CGS = 3,
+  MTLGPU_BICGSTAB_2 = 4,
+  MTLGPU_BICGSTAB_ELL = 5,
+  MTLGPU_TFQMR = 6,
+  MTLGPU_QMR = 7,
+  MTLGPU_IDR_S = 8,
+  MTLGPU_GMRES = 9
+} mtlgpu_method;
 
 /* Solve modes.
  *  FP64         : the reference's arithmetic throughout (iteration counts
@@ -357,6 +370,33 @@ mtlgpu_status mtlgpu_solve_host(int method, mtlgpu_csr* A, mtlgpu_pc* P, double*
                                 const double* h_b, const mtlgpu_iter_params* params,
                                 mtlgpu_iter_result* res);
 void mtlgpu_iter_params_default(mtlgpu_iter_params* p);
+
+/* The other ITL Krylov methods with a left preconditioner L and a right
+ * preconditioner R (either may be NULL: identity), as the reference calls
+ * them:
+ *   MTLGPU_BICG          itl::bicg(A, x, b, L, iter)               (R unused)
+ *   MTLGPU_CGS           itl::cgs(A, x, b, L, iter)                (R unused)
+ *   MTLGPU_BICGSTAB_2    itl::bicgstab_2(A, x, b, L, iter)         (R unused)
+ *   MTLGPU_BICGSTAB_ELL  itl::bicgstab_ell(A, x, b, L, R, iter, l) param = l (0: 8; <= 32)
+ *   MTLGPU_TFQMR         itl::tfqmr(A, x, b, L, R, iter)
+ *   MTLGPU_QMR           itl::qmr(A, x, b, L, R, iter)
+ *   MTLGPU_IDR_S         itl::idr_s(A, x, b, L, R, iter, s)        param = s (0: 8; <= 15);
+ *                        L and R are ignored, as by the reference; the random
+ *                        shadow space is drawn as the reference draws it in a
+ *                        fresh process (srand(17 (k + 2)) and rand() for
+ *                        vector k), which reseeds the C library's generator
+ *   MTLGPU_GMRES         itl::gmres(A, x, b, L, R, iter, restart)  param = restart (0: 8; <= 64)
+ * (MTLGPU_CG / MTLGPU_BICGSTAB are mtlgpu_solve.)  FP64 only (params->mode
+ * must be MTLGPU_SOLVE_FP64), preconditioners with FP64 factors.  The
+ * iteration control and residual history follow basic_iteration as in
+ * mtlgpu_solve.  A breakdown branch of the reference (`return
+ * iter.fail(code, ...)`, and cgs's zero rho that only records code 2;
+ * idr_s's matrix_singular) returns MTLGPU_BREAKDOWN with res->error = the
+ * reference's code.  An empty system is MTLGPU_INVALID_ARG for the methods
+ * whose reference throws "empty rhs vector". */
+mtlgpu_status mtlgpu_solve_krylov(int method, mtlgpu_csr* A, mtlgpu_pc* L, mtlgpu_pc* R,
+                                  int param, double* d_x, const double* d_b,
+                                  const mtlgpu_iter_params* params, mtlgpu_iter_result* res);
 
 /* Batched PCG: `count` independent systems in one solve.  Each system s is
  * the diagonal block of rows/columns [h_offsets[s], h_offsets[s+1]) of the

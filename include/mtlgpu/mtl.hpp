@@ -980,6 +980,54 @@ int solve(int method, const compressed2D<double>& A, dense_vector<double>& x,
   return iter;
 }
 
+/// The other Krylov methods (mtlgpu_solve_krylov).  The device records every
+/// residual the reference's loop passes to finished(); they are replayed
+/// through `iter` one per iteration after the first (bicg, cgs: finished(r0),
+/// then ++iter, finished(r_k)); for the methods that test several times per
+/// iteration or at the top of their loop, the iteration object is advanced
+/// to the device's count and given the last residual.  A breakdown returns
+/// iter.fail(code) as the reference does; idr_s's singular LU raises
+/// mtl::runtime_error ("matrix singular").
+template <typename Iteration>
+int solve_krylov(int method, const compressed2D<double>& A, dense_vector<double>& x,
+                 const dense_vector<double>& b, mtlgpu_pc* L, mtlgpu_pc* R, int param,
+                 Iteration& iter) {
+  typedef typename Iteration::real Real;
+  if (A.num_rows() != A.num_cols()) throw mtl::matrix_not_square();
+  if (x.size() != A.num_cols() || b.size() != A.num_rows()) throw mtl::incompatible_size();
+  mtlgpu_iter_params p;
+  mtlgpu_iter_params_default(&p);
+  p.max_iter = iter.max_iterations() - iter.iterations();
+  p.rtol = iter.tol();
+  p.atol = iter.atol();
+  p.norm_r0 = iter.norm_r0();
+  std::vector<double> hist(size_t(param + 4) * size_t(p.max_iter > 0 ? p.max_iter + 2 : 2));
+  p.h_resid_history = hist.data();
+  p.history_cap = int(hist.size());
+  mtlgpu_iter_result res;
+  const int st = mtlgpu_solve_krylov(method, A.handle(), L, R, param, x.data(), b.data(), &p,
+                                     &res);
+  if (st != MTLGPU_OK && st != MTLGPU_MAX_ITER && st != MTLGPU_BREAKDOWN)
+    throw_on(st, A.ctx().get());
+  const int n_hist = std::min(res.history_len, int(hist.size()));
+  if (method == MTLGPU_BICG || method == MTLGPU_CGS) {
+    bool done = n_hist == 0 || iter.finished(Real(hist[0]));
+    for (int k = 1; !done && k < n_hist; ++k) {
+      ++iter;
+      done = iter.finished(Real(hist[k]));
+    }
+    while (iter.iterations() < res.iterations) ++iter;  // breakdown inside an iteration
+  } else {
+    iter += res.iterations;
+    iter.finished(Real(res.resid));
+  }
+  if (st == MTLGPU_BREAKDOWN) {
+    if (method == MTLGPU_IDR_S) throw mtl::runtime_error("matrix singular");
+    return iter.fail(res.error);
+  }
+  return iter;
+}
+
 }  // namespace detail
 }  // namespace gpu
 
@@ -1189,6 +1237,69 @@ int bicgstab(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<dou
              const mtl::gpu::refinement& how) {
   return mtl::gpu::detail::solve(MTLGPU_BICGSTAB, A, x, b, mtl::gpu::detail::pc_handle(P), iter,
                                  &how);
+}
+
+/// itl::bicg(A, x, b, M, iter) on the device (itl/krylov/bicg.hpp:22-63).
+template <typename Preconditioner, typename Iteration>
+int bicg(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+         const mtl::gpu::dense_vector<double>& b, const Preconditioner& P, Iteration& iter) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_BICG, A, x, b, mtl::gpu::detail::pc_handle(P),
+                                        nullptr, 0, iter);
+}
+/// itl::cgs(A, x, b, M, iter) (itl/krylov/cgs.hpp:23-65).
+template <typename Preconditioner, typename Iteration>
+int cgs(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+        const mtl::gpu::dense_vector<double>& b, const Preconditioner& P, Iteration& iter) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_CGS, A, x, b, mtl::gpu::detail::pc_handle(P),
+                                        nullptr, 0, iter);
+}
+/// itl::bicgstab_2(A, x, b, L, iter) (itl/krylov/bicgstab_2.hpp:33-131).
+template <typename Preconditioner, typename Iteration>
+int bicgstab_2(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+               const mtl::gpu::dense_vector<double>& b, const Preconditioner& L, Iteration& iter) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_BICGSTAB_2, A, x, b,
+                                        mtl::gpu::detail::pc_handle(L), nullptr, 2, iter);
+}
+/// itl::bicgstab_ell(A, x, b, L, R, iter, l) (itl/krylov/bicgstab_ell.hpp:37-132).
+template <typename LeftPreconditioner, typename RightPreconditioner, typename Iteration>
+int bicgstab_ell(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+                 const mtl::gpu::dense_vector<double>& b, const LeftPreconditioner& L,
+                 const RightPreconditioner& R, Iteration& iter, size_t l) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_BICGSTAB_ELL, A, x, b,
+                                        mtl::gpu::detail::pc_handle(L),
+                                        mtl::gpu::detail::pc_handle(R), int(l), iter);
+}
+/// itl::tfqmr(A, x, b, L, R, iter) (itl/krylov/tfqmr.hpp:26-100).
+template <typename LeftPreconditioner, typename RightPreconditioner, typename Iteration>
+int tfqmr(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+          const mtl::gpu::dense_vector<double>& b, const LeftPreconditioner& L,
+          const RightPreconditioner& R, Iteration& iter) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_TFQMR, A, x, b, mtl::gpu::detail::pc_handle(L),
+                                        mtl::gpu::detail::pc_handle(R), 0, iter);
+}
+/// itl::qmr(A, x, b, L, R, iter) (itl/krylov/qmr.hpp:24-109).
+template <typename LeftPreconditioner, typename RightPreconditioner, typename Iteration>
+int qmr(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+        const mtl::gpu::dense_vector<double>& b, LeftPreconditioner& L,
+        const RightPreconditioner& R, Iteration& iter) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_QMR, A, x, b, mtl::gpu::detail::pc_handle(L),
+                                        mtl::gpu::detail::pc_handle(R), 0, iter);
+}
+/// itl::idr_s(A, x, b, L, R, iter, s) (itl/krylov/idr_s.hpp:30-105); both
+/// preconditioners are ignored, as by the reference.
+template <typename LeftPreconditioner, typename RightPreconditioner, typename Iteration>
+int idr_s(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+          const mtl::gpu::dense_vector<double>& b, const LeftPreconditioner&,
+          const RightPreconditioner&, Iteration& iter, size_t s) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_IDR_S, A, x, b, nullptr, nullptr, int(s), iter);
+}
+/// itl::gmres(A, x, b, L, R, iter, restart) (itl/krylov/gmres.hpp:121-135).
+template <typename LeftPreconditioner, typename RightPreconditioner, typename Iteration>
+int gmres(const mtl::gpu::compressed2D<double>& A, mtl::gpu::dense_vector<double>& x,
+          const mtl::gpu::dense_vector<double>& b, LeftPreconditioner& L, RightPreconditioner& R,
+          Iteration& iter, typename mtl::Collection<mtl::gpu::dense_vector<double>>::size_type restart) {
+  return mtl::gpu::detail::solve_krylov(MTLGPU_GMRES, A, x, b, mtl::gpu::detail::pc_handle(L),
+                                        mtl::gpu::detail::pc_handle(R), int(restart), iter);
 }
 
 }  // namespace itl

@@ -601,10 +601,29 @@ void mtlgpu_iter_params_default(mtlgpu_iter_params* p) {
   p->inner_rtol = 1e-4;
 }
 
+mtlgpu_status mtlgpu_solve_krylov(int method, mtlgpu_csr* A, mtlgpu_pc* L, mtlgpu_pc* R,
+                                  int param, double* x, const double* b,
+                                  const mtlgpu_iter_params* prm, mtlgpu_iter_result* res) {
+  if (!A || !prm || !res || (A->n_rows && (!x || !b)) || prm->max_iter < 0 || param < 0)
+    return MTLGPU_INVALID_ARG;
+  if (method == MTLGPU_CG || method == MTLGPU_BICGSTAB) {
+    if (R) return MTLGPU_INVALID_ARG;  // cg / bicgstab take one preconditioner
+    return mtlgpu_solve(method, A, L, x, b, prm, res);
+  }
+  MTLGPU_TRY(set_device(A->ctx));
+  const long long launches_before = A->ctx->launches;
+  mtlgpu_status s = solve_krylov_impl(method, A, L, R, param, x, b, prm, res);
+  res->status = s;
+  res->kernel_launches = A->ctx->launches - launches_before;
+  return s;
+}
+
 mtlgpu_status mtlgpu_solve(int method, mtlgpu_csr* A, mtlgpu_pc* P, double* x, const double* b,
                            const mtlgpu_iter_params* prm, mtlgpu_iter_result* res) {
   if (!A || !prm || !res || (A->n_rows && (!x || !b)) || prm->max_iter < 0)
     return MTLGPU_INVALID_ARG;
+  if (method >= MTLGPU_BICG && method <= MTLGPU_GMRES)
+    return mtlgpu_solve_krylov(method, A, P, nullptr, 0, x, b, prm, res);
   MTLGPU_TRY(set_device(A->ctx));
   const long long launches_before = A->ctx->launches;
   mtlgpu_status s = solve_impl(method, A, P, x, b, prm, res);

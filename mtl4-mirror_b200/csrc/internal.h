@@ -71,6 +71,7 @@ struct Sell {
 };
 
 struct Pc;
+struct XWork;  // workspace of the other Krylov methods (krylov_ext.cu)
 // Solver workspace cache entry (buffers + instantiated graph; krylov.cu).
 struct WorkspaceEntry {
   Pc* P;
@@ -81,6 +82,7 @@ struct WorkspaceEntry {
 struct Csr {
   Ctx* ctx = nullptr;
   std::vector<WorkspaceEntry> workspaces;
+  std::vector<XWork*> xwork;
   int n_rows = 0, n_cols = 0, nnz = 0;
   int32_t* d_rp = nullptr;
   int32_t* d_ci = nullptr;
@@ -302,6 +304,12 @@ mtlgpu_status pc_apply_t(Pc* P, const T* r, T* z, bool adjoint, const int* skip,
 mtlgpu_status dot_launch(Ctx* ctx, int n, const double* x, const double* y, double* d_out,
                          int order);
 mtlgpu_status axpby_launch(Ctx* ctx, int n, double alpha, const double* x, double beta, double* y);
+
+// The other Krylov methods (krylov_ext.cu)
+mtlgpu_status solve_krylov_impl(int method, Csr* A, Pc* L, Pc* R, int param, double* d_x,
+                                const double* d_b, const mtlgpu_iter_params* prm,
+                                mtlgpu_iter_result* res);
+void release_xwork(Csr* A, const Pc* only_P);
 
 // Krylov driver (krylov.cu)
 mtlgpu_status solve_impl(int method, Csr* A, Pc* P, double* d_x, const double* d_b,

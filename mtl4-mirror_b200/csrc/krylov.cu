@@ -863,6 +863,7 @@ mtlgpu_status true_residual(Csr* A, const double* x, const double* b, double* sc
 
 void release_workspaces(Csr* A, Pc* only_P) {
   release_batch_work(A, only_P);
+  release_xwork(A, only_P);
   std::vector<WorkspaceEntry> keep;
   for (auto& e : A->workspaces) {
     if (only_P && e.P != only_P) {

@@ -679,9 +679,13 @@ mtlgpu_status part_plan_build(Ctx* ctx, SweepPlan* S, bool with_fp32) {
   const int n = S->n;
   if (n == 0 || ctx->part_sweeps == 0) return MTLGPU_OK;
   // automatic choice: the partitioned sweep where levels are narrow (few rows
-  // per level, long dependency chains: 2-D grids, where it measured 16 %
-  // faster); the level-ordered ticket sweep where levels are wide (3-D grids)
-  if (ctx->part_sweeps == 2 && (S->n_levels == 0 || n / S->n_levels > kAutoRowsPerLevel))
+  // per level, long dependency chains) and factor rows short (2-D 5-point
+  // grids, where it measured 16 % faster); the level-ordered ticket sweep
+  // where levels are wide (3-D grids) or rows long (27-point factors: 5.7 ms
+  // partitioned against under 1 ms for the ticket sweep at 48^3)
+  if (ctx->part_sweeps == 2 &&
+      (S->n_levels == 0 || n / S->n_levels > kAutoRowsPerLevel ||
+       (long long)S->nnz_off * 2 > 5ll * n))
     return MTLGPU_OK;
 
   // host copies of the level-ordered plan

@@ -26,8 +26,10 @@ OK, MAX_ITER, INVALID_ARG, NOT_SQUARE, MISSING_DIAGONAL, ZERO_PIVOT, BREAKDOWN, 
 FP64, FP32 = 0, 1
 PC_IDENTITY, PC_DIAGONAL, PC_ILU0, PC_IC0 = range(4)
 PC_KINDS = {"identity": PC_IDENTITY, "diagonal": PC_DIAGONAL, "ilu0": PC_ILU0, "ic0": PC_IC0}
-CG, BICGSTAB = 0, 1
-METHODS = {"cg": CG, "bicgstab": BICGSTAB}
+CG, BICGSTAB, BICG, CGS, BICGSTAB_2, BICGSTAB_ELL, TFQMR, QMR, IDR_S, GMRES = range(10)
+METHODS = {"cg": CG, "bicgstab": BICGSTAB, "bicg": BICG, "cgs": CGS, "bicgstab_2": BICGSTAB_2,
+           "bicgstab_ell": BICGSTAB_ELL, "tfqmr": TFQMR, "qmr": QMR, "idr_s": IDR_S,
+           "gmres": GMRES}
 SOLVE_FP64, SOLVE_MIXED = 0, 1
 LOWER, UPPER = 0, 1
 UPDATE_STORE, UPDATE_PLUS, UPDATE_MINUS, UPDATE_TIMES = range(4)
@@ -445,6 +447,20 @@ def solve(method, A, P, x, b, **kw):
     res = IterResult()
     st = _lib().mtlgpu_solve(METHODS.get(method, method), A.h, P.h if P else None, x.ptr, b.ptr,
                              C.byref(prm), C.byref(res))
+    return st, res, hist[:min(res.history_len, len(hist))].copy()
+
+
+def solve_krylov(method, A, L, x, b, R=None, param=0, **kw):
+    """mtlgpu_solve_krylov: bicg / cgs / bicgstab_2 / bicgstab_ell / tfqmr /
+    qmr / idr_s / gmres with left preconditioner L and right preconditioner R
+    (None: identity) on device arrays; returns (status, IterResult, history)."""
+    max_iter = kw.get("max_iter", 1000)
+    hist = np.zeros((max(param, 2) + 3) * (max_iter + 2) + 16)
+    prm = make_params(history=hist, **kw)
+    res = IterResult()
+    st = _lib().mtlgpu_solve_krylov(METHODS.get(method, method), A.h, L.h if L else None,
+                                    R.h if R else None, int(param), x.ptr, b.ptr, C.byref(prm),
+                                    C.byref(res))
     return st, res, hist[:min(res.history_len, len(hist))].copy()
 
 

@@ -178,6 +178,10 @@ class _Base:
                     history=hist[:min(cnt, cap)].copy())
 
 
+KRYLOV = {"bicg": 2, "cgs": 3, "bicgstab_2": 4, "bicgstab_ell": 5, "tfqmr": 6, "qmr": 7,
+          "idr_s": 8, "gmres": 9}
+
+
 class Restatement(_Base):
     prefix = "or_"
 
@@ -265,6 +269,29 @@ class Reference(_Base):
 
     def threads(self):
         return int(self.lib.ref_omp_threads())
+
+    def solve_krylov(self, method, pc_left, A, b, pc_right="identity", param=0, x0=None,
+                     max_iter=1000, rtol=1e-10, atol=0.0, norm_r0=-1.0, hist_cap=None):
+        """The reference's bicg / cgs / bicgstab_2 / bicgstab_ell / tfqmr / qmr /
+        idr_s / gmres (ref_solve_krylov).  Same result dict as solve()."""
+        n, rp, ci, v = A
+        method = KRYLOV.get(method, method)
+        pl, pr = PC_NAMES.get(pc_left, pc_left), PC_NAMES.get(pc_right, pc_right)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(n) if x0 is None else np.array(x0, np.float64, copy=True)
+        cap = (4 * max_iter + 16) if hist_cap is None else hist_cap
+        hist = np.zeros(max(cap, 1))
+        out = np.zeros(6)
+        f = self._f("solve_krylov")
+        f.restype = C.c_int
+        err = f(C.c_int(method), C.c_int(pl), C.c_int(pr), C.c_int(param), C.c_int(n),
+                C.c_int(len(ci)), _ptr(rp), _ptr(ci), _ptr(v), _ptr(b), _ptr(x),
+                C.c_int(max_iter), C.c_double(rtol), C.c_double(atol), C.c_double(norm_r0),
+                _ptr(hist), C.c_int(cap), _ptr(out))
+        cnt = int(out[5])
+        return dict(err=err, x=x, iterations=int(out[0]), resid=float(out[1]),
+                    norm_r0=float(out[2]), t_factor=float(out[3]), t_solve=float(out[4]),
+                    history=hist[:min(cnt, cap)].copy())
 
     def spmv_time(self, A, x, reps):
         n, rp, ci, v = A

@@ -360,6 +360,81 @@ int ref_assemble(int n_rows, int n_cols, int base_nnz, const int* brp, const int
   return export_csr(A, rp, ci, v);
 }
 
+// The other ITL Krylov methods, called as the reference's tests call them:
+//   method 2 bicg(A, x, b, L, iter)                     itl/krylov/bicg.hpp:22-63
+//          3 cgs(A, x, b, L, iter)                      itl/krylov/cgs.hpp:23-65
+//          4 bicgstab_2(A, x, b, L, iter)               itl/krylov/bicgstab_2.hpp:33-131
+//          5 bicgstab_ell(A, x, b, L, R, iter, param)   itl/krylov/bicgstab_ell.hpp:37-132
+//          6 tfqmr(A, x, b, L, R, iter)                 itl/krylov/tfqmr.hpp:26-100
+//          7 qmr(A, x, b, L, R, iter)                   itl/krylov/qmr.hpp:24-109
+//          8 idr_s(A, x, b, L, R, iter, param)          itl/krylov/idr_s.hpp:30-105
+//          9 gmres(A, x, b, L, R, iter, param)          itl/krylov/gmres.hpp:121-135
+// pc_left / pc_right: 0 identity, 1 diagonal, 2 ilu_0, 3 ic_0.  idr_s's
+// random shadow space is drawn as in a fresh process (mtl::seed counter
+// reset to 0 before the call, mtl/operation/random.hpp:27-37).  Returns and
+// fills out[] as ref_solve does.
+int ref_solve_krylov(int method, int pc_left, int pc_right, int param, int n, int nnz,
+                     const int* rp, const int* ci, const double* v, const double* b, double* x,
+                     int max_iter, double rtol, double atol, double norm_r0, double* hist,
+                     int hist_cap, double* out) {
+  matrix_type A = make_matrix(n, nnz, rp, ci, v);
+  vector_type bv = make_vector(n, b), xv = make_vector(n, x);
+  if (norm_r0 < 0) norm_r0 = two_norm(bv);
+  recording_iteration iter(norm_r0, max_iter, rtol, atol, hist, hist_cap);
+  int err = 0;
+  double tf = 0, ts = 0;
+  auto with_pc = [&](int kind, auto&& body) {
+    switch (kind) {
+      case PC_IDENTITY: { itl::pc::identity<matrix_type> P(A); body(P); break; }
+      case PC_DIAGONAL: { itl::pc::diagonal<matrix_type> P(A); body(P); break; }
+      case PC_ILU0: { itl::pc::ilu_0<matrix_type> P(A); body(P); break; }
+      case PC_IC0: { itl::pc::ic_0<matrix_type> P(A); body(P); break; }
+      default: err = -4;
+    }
+  };
+  try {
+    auto t0 = std::chrono::steady_clock::now();
+    with_pc(pc_left, [&](auto& L) {
+      with_pc(pc_right, [&](auto& R) {
+        tf = seconds_since(t0);
+        t0 = std::chrono::steady_clock::now();
+        const size_t prm = size_t(param);
+        switch (method) {
+          case 2: err = itl::bicg(A, xv, bv, L, iter); break;
+          case 3: err = itl::cgs(A, xv, bv, L, iter); break;
+          case 4: err = itl::bicgstab_2(A, xv, bv, L, iter); break;
+          case 5: err = itl::bicgstab_ell(A, xv, bv, L, R, iter, prm ? prm : 8); break;
+          case 6: err = itl::tfqmr(A, xv, bv, L, R, iter); break;
+          case 7: err = itl::qmr(A, xv, bv, L, R, iter); break;
+          case 8:
+            mtl::seed<double>::counter = 0;
+            err = itl::idr_s(A, xv, bv, L, R, iter, prm ? prm : 8);
+            break;
+          case 9: err = itl::gmres(A, xv, bv, L, R, iter, prm ? prm : 8); break;
+          default: err = -4;
+        }
+        ts = seconds_since(t0);
+      });
+    });
+  } catch (itl::unexpected_orthogonality&) {
+    err = -2;
+  } catch (mtl::runtime_error&) {
+    err = -3;
+  } catch (mtl::logic_error&) {
+    err = -3;
+  }
+  store_vector(xv, x);
+  if (out) {
+    out[0] = iter.iterations();
+    out[1] = iter.resid();
+    out[2] = norm_r0;
+    out[3] = tf;
+    out[4] = ts;
+    out[5] = iter.count;
+  }
+  return err;
+}
+
 // Build-flavour tag, so callers can report how the baseline was compiled.
 const char* ref_build_info(void) {
 #ifdef MTL_WITH_OPENMP

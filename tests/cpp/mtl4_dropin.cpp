@@ -151,6 +151,57 @@ void case_pc() {
               max_abs_diff(y, dy), max_abs_diff(yi, dyi), max_abs_diff(ya, dya));
 }
 
+// The other Krylov methods called exactly as the reference's tests call them,
+// on mtl::compressed2D (CPU) and on mtl::gpu::compressed2D (device), ILU(0)
+// on the left, identity on the right, 27-point convection-diffusion 6^3.
+void case_krylov() {
+  const int N = 6, n = N * N * N;
+  const long long nnz = mtlgpu_gen_convdiff27(N, 2, nullptr, nullptr, nullptr);
+  std::vector<int32_t> rp(n + 1), ci(nnz);
+  std::vector<double> v(nnz);
+  mtlgpu_gen_convdiff27(N, 2, rp.data(), ci.data(), v.data());
+  std::vector<std::size_t> rps(rp.begin(), rp.end()), cis(ci.begin(), ci.end());
+  Matrix A(n, n, std::size_t(nnz), rps.data(), cis.data(), v.data());
+  Vector xt = uniform(n, 1), b(n);
+  b = A * xt;
+  DMatrix dA(A);
+  DVector db(b);
+  itl::pc::ilu_0<Matrix> L(A);
+  itl::pc::identity<Matrix> R(A);
+  itl::pc::ilu_0<DMatrix> dL(dA);
+  itl::pc::identity<DMatrix> dR(dA);
+  const char* names[] = {"bicg", "cgs", "bicgstab_2", "bicgstab_ell", "tfqmr", "qmr", "idr_s",
+                         "gmres"};
+  std::printf("{\"case\": \"krylov\"");
+  for (int m = 0; m < 8; ++m) {
+    const int max_it = m == 5 ? 60 : 400;
+    Vector x(n, 0.0);
+    DVector dx(n, 0.0);
+    itl::basic_iteration<double> it(b, max_it, 1.e-8), dit(b, max_it, 1.e-8);
+    int e = 0, de = 0;
+    switch (m) {
+      case 0: e = itl::bicg(A, x, b, L, it); de = itl::bicg(dA, dx, db, dL, dit); break;
+      case 1: e = itl::cgs(A, x, b, L, it); de = itl::cgs(dA, dx, db, dL, dit); break;
+      case 2: e = itl::bicgstab_2(A, x, b, L, it); de = itl::bicgstab_2(dA, dx, db, dL, dit); break;
+      case 3:
+        e = itl::bicgstab_ell(A, x, b, L, R, it, 4);
+        de = itl::bicgstab_ell(dA, dx, db, dL, dR, dit, 4);
+        break;
+      case 4: e = itl::tfqmr(A, x, b, L, R, it); de = itl::tfqmr(dA, dx, db, dL, dR, dit); break;
+      case 5: e = itl::qmr(A, x, b, L, R, it); de = itl::qmr(dA, dx, db, dL, dR, dit); break;
+      case 6:
+        mtl::seed<double>::counter = 0;
+        e = itl::idr_s(A, x, b, L, R, it, 2);
+        de = itl::idr_s(dA, dx, db, dL, dR, dit, 2);
+        break;
+      case 7: e = itl::gmres(A, x, b, L, R, it, 8); de = itl::gmres(dA, dx, db, dL, dR, dit, 8); break;
+    }
+    std::printf(", \"%s\": {\"cpu\": [%d, %d], \"gpu\": [%d, %d], \"x_max_diff\": %.3g}",
+                names[m], it.iterations(), e, dit.iterations(), de, max_abs_diff(x, dx));
+  }
+  std::printf("}\n");
+}
+
 // The same insertion code on mtl::compressed2D (the reference's inserter)
 // and on mtl::gpu::compressed2D (assembled on the device): seeded triplets
 // with duplicates, `<<` with update_plus, `=` and `+=` mixed, into a matrix
@@ -215,8 +266,9 @@ int main(int argc, char** argv) {
     else if (c == "bicgstab") case_bicgstab();
     else if (c == "pc") case_pc();
     else if (c == "assemble") case_assemble();
+    else if (c == "krylov") case_krylov();
     else {
-      std::fprintf(stderr, "usage: mtl4_dropin cg|bicgstab|pc|assemble\n");
+      std::fprintf(stderr, "usage: mtl4_dropin cg|bicgstab|pc|assemble|krylov\n");
       return 2;
     }
   } catch (const std::exception& e) {

@@ -12,7 +12,7 @@ Run in a checkout where the reference tree is present (it is compiled by
 
 Every array stored here is an output of the reference's own code path
 (laplacian_setup, compressed2D SpMV, the compressed2D inserter, ic_0 /
-ilu_0 factors, solve(P, x),
+ilu_0 factors, solve(P, x), the other ITL Krylov methods,
 itl::cg / itl::bicgstab with basic_iteration), except the level arrays,
 which the reference does not compute: those come from the restatement
 (oracle/restate.c, or_levels_lower/upper) applied to the reference's own
@@ -160,6 +160,56 @@ def assembly_cases(R, out):
     out["asm_mix_rp"], out["asm_mix_ci"], out["asm_mix_v"] = rp, ci, v
 
 
+KRYLOV_METHODS = ["bicg", "cgs", "bicgstab_2", "bicgstab_ell", "tfqmr", "qmr", "idr_s", "gmres"]
+KRYLOV_PCS = [("identity", "identity"), ("ilu0", "identity"), ("diagonal", "ilu0"),
+              ("ic0", "diagonal")]
+
+
+def krylov_problems():
+    """The small systems the other Krylov methods are pinned on: 27-point
+    convection-diffusion 6^3 (unsymmetric), the 12 x 12 Laplacian and the
+    16 x 16 finite-volume operator; b = A x_true, x_true ~ U[-1,1] seed 1."""
+    return [("cd6", M.convdiff27(6, 2)), ("lap12", M.laplacian2d(12, 12)),
+            ("fv16", M.fv2d(16, 1.0, 8.0, 4))]
+
+
+def krylov_param(method):
+    return {"bicgstab_ell": 4, "idr_s": 2, "gmres": 8}.get(method, 0)
+
+
+def krylov_max_iter(method):
+    return 60 if method == "qmr" else 400
+
+
+def krylov_cases(R, out):
+    """The reference's bicg, cgs, bicgstab_2, bicgstab_ell (l = 4), tfqmr, qmr
+    (60 iterations: its test on the Lanczos norm never stops it earlier),
+    idr_s (s = 2) and gmres (restart 8) with left / right preconditioners, to
+    rtol 1e-8: [iterations, error], the last residual tested, x, and the
+    first 64 residuals recorded."""
+    for name, A in krylov_problems():
+        b = R.spmv(A, M.uniform(A[0], 1))
+        out[f"kry_{name}_b"] = b
+        for meth in KRYLOV_METHODS:
+            for pl, pr in KRYLOV_PCS:
+                r = R.solve_krylov(meth, pl, A, b, pc_right=pr, param=krylov_param(meth),
+                                   max_iter=krylov_max_iter(meth), rtol=1e-8)
+                key = f"kry_{name}_{meth}_{pl}_{pr}"
+                out[key + "_iters"] = np.array([r["iterations"], r["err"]])
+                out[key + "_resid"] = np.array([r["resid"], r["norm_r0"]])
+                out[key + "_x"] = r["x"]
+                out[key + "_hist"] = r["history"][:64]
+    # gmres and idr_s cut after a few cycles / steps on cd6 (no preconditioner)
+    A = M.convdiff27(6, 2)
+    b = out["kry_cd6_b"]
+    for meth, cuts in (("gmres", (8, 16, 24, 32)), ("idr_s", (1, 2, 3, 5, 8, 13))):
+        for k in cuts:
+            r = R.solve_krylov(meth, "identity", A, b, param=krylov_param(meth), max_iter=k,
+                               rtol=1e-8)
+            out[f"kry_cut_{meth}_{k}_x"] = r["x"]
+            out[f"kry_cut_{meth}_{k}_resid"] = np.array([r["resid"], r["iterations"]])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cfg2", action="store_true")
@@ -239,6 +289,7 @@ def main():
         out[f"rg_{pc}_hist"] = rr["history"]
 
     assembly_cases(R, out)
+    krylov_cases(R, out)
 
     # 2-D finite volume, 32^2 (seed 4)
     A = M.fv2d(32, 1.0, 8.0, 4)

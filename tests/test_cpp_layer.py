@@ -160,3 +160,17 @@ def test_mtl4_dropin_inserter():
     _dropin()
     r = _run("mtl4_dropin", "assemble")
     assert r["identical"] and r["laplacian_identical"] and r["nnz"] > 0
+
+
+@pytest.mark.gpu
+def test_mtl4_dropin_other_krylov_methods():
+    # itl::bicg ... itl::gmres called as the reference's tests call them, on
+    # the reference's CPU types and on device types in one program
+    _dropin()
+    r = _run("mtl4_dropin", "krylov")
+    for meth in ("bicg", "cgs", "bicgstab_2", "bicgstab_ell", "tfqmr", "qmr", "idr_s", "gmres"):
+        cpu, gpu = r[meth]["cpu"], r[meth]["gpu"]
+        assert cpu[1] == gpu[1], (meth, cpu, gpu)
+        tol = 8 if meth == "gmres" else 2
+        assert abs(cpu[0] - gpu[0]) <= tol, (meth, cpu, gpu)
+        assert r[meth]["x_max_diff"] <= 1e-5, (meth, r[meth])

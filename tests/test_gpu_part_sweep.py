@@ -73,6 +73,9 @@ def test_automatic_sweep_choice(M, ctx):
     assert P2.sweep_kind(M.LOWER) == 1 and P2.sweep_kind(M.UPPER) == 1
     P3 = M.Pc(M.Csr(ctx, *M.laplacian3d(64)[1:]), "ic0")
     assert P3.sweep_kind(M.LOWER) == 0
+    # long factor rows (27-point ILU(0), 13 off-diagonal entries a row): ticket
+    P4 = M.Pc(M.Csr(ctx, *M.convdiff27(48, 2)[1:]), "ilu0")
+    assert P4.sweep_kind(M.LOWER) == 0 and P4.sweep_kind(M.UPPER) == 0
 
 
 def test_part_sweep_timeout_leaves_context_usable(M, ctx):
