@@ -198,15 +198,15 @@ def run_reference_arm(args, rank):
 
 def cpu_baseline(M, A, b, A3, b3):
     """The reference's CPU path on the host cores (rank 0, N = 1): the full
-    FP64 PCG-IC(0) solve (median of 3, OpenMP build; 1 run of the serial
-    build), ic_0 factorisation (median of 3), one SpMV (mean over 1000 reps
+    FP64 PCG-IC(0) solve (median of 5, OpenMP build; 1 run of the serial
+    build), ic_0 factorisation (median of 5), one SpMV (mean over 1000 reps
     with OpenMP, 100 serial: the sparse_matrix_vector_timing.cpp protocol), and
     config 3's bicgstab + ilu_0 solve (OpenMP build)."""
     ref, kind, cores = reference_solver("omp")
     out = {"unit": "ms", "cores": cores, "kind": kind, "cpu_model": cpu_model(),
            "nproc": os.cpu_count()}
     time_reference_solve(ref, kind, A, b)   # warm-up
-    runs = [time_reference_solve(ref, kind, A, b) for _ in range(3)]
+    runs = [time_reference_solve(ref, kind, A, b) for _ in range(5)]
     out["value"] = 1e3 * statistics.median(r[0] for r in runs)
     out["ic0_factor_ms"] = 1e3 * statistics.median(r[2] for r in runs)
     iters = runs[-1][1]
@@ -226,6 +226,23 @@ def cpu_baseline(M, A, b, A3, b3):
     # the reference's inserter on the same shuffled triplets (slot size 7, one
     # run): mtl::mat::inserter<compressed2D> from construction to destruction
     if kind == "reference":
+        # config 4: the reference's itl::cg looped over the same 512 systems
+        # (diagonal and ic_0, FP64 to 1e-8), one run each; solve and
+        # factorisation times summed separately
+        systems, (nb_, _, _, _, offb) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2, seed=3)
+        bb = M.normal(nb_, 3)
+        bat = {}
+        for pc in ("diagonal", "ic0"):
+            ts = tf = 0.0
+            its = []
+            for s_, As in enumerate(systems):
+                rr = ref.solve("cg", pc, As, bb[offb[s_]:offb[s_ + 1]], rtol=1e-8, max_iter=5000)
+                ts += rr["t_solve"]
+                tf += rr["t_factor"]
+                its.append(rr["iterations"])
+            bat[pc] = {"solve_ms": 1e3 * ts, "factor_ms": 1e3 * tf, "iterations_max": max(its),
+                       "iterations_mean": float(np.mean(its))}
+        out["batched_512_systems"] = bat
         # the other Krylov methods on the same 48^3 system as the device leg
         Ak, bk = krylov_system(M)
         kr = {}
@@ -238,9 +255,11 @@ def cpu_baseline(M, A, b, A3, b3):
         ref.assemble(A[0], A[0], r_, c_, v_, slot_size=7)
         out["assembly_inserter_ms"] = 1e3 * ref.last_seconds
     out["sample"] = (f"full FP64 PCG-IC(0) solves to 1e-10 ({iters} iterations) of the same "
-                     "system, median of 3 after 1 warm-up (OpenMP build, all host threads); "
+                     "system, median of 5 after 1 warm-up (OpenMP build, all host threads); "
                      "factorisation timed separately; SpMV 1000 reps (OpenMP) / 100 reps "
-                     "(serial); config 3: one FP64 bicgstab + ilu_0 solve (OpenMP); assembly: one "
+                     "(serial); config 3: one FP64 bicgstab + ilu_0 solve (OpenMP); config 4: "
+                     "itl::cg over the 512 systems, one run each, diagonal and ic_0; the "
+                     "other Krylov methods on 27-point 48^3, one run each; assembly: one "
                      "inserter run over the 14.6M shuffled triplets of the 128^3 matrix")
     return out
 
@@ -486,7 +505,25 @@ def adjoint_workload(M, ctx, stream):
     ms_b, rb = _local_ms(backward, 2, stream)
     out = {"n": int(n), "nnz": int(len(ci)), "forward_ms": ms_f, "backward_ms": ms_b,
            "forward_iterations": rf[-1].iterations, "backward_iterations": rb[-1].iterations,
-           "dtype": "f64", "rtol": 1e-10}
+           "dtype": "f64", "rtol": 1e-10, "pc": "IC(0), exact triangular solves"}
+    x_ex, g_ex, l_ex = dx.download(), grad.download(), dlam.download()
+    # the same FP64 solves with the IC(0) factors applied by k Jacobi
+    # iterations per triangle: another preconditioner, the same gradients to
+    # the solve tolerance
+    for k in (1, 2):
+        P.set_jacobi_sweeps(k)
+        forward()
+        backward()
+        mf, rf = _local_ms(forward, 2, stream)
+        mb, rb = _local_ms(backward, 2, stream)
+        xk, gk, lk = dx.download(), grad.download(), dlam.download()
+        rel = lambda a, b_: float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
+        out[f"jacobi_k{k}"] = {"forward_ms": mf, "backward_ms": mb,
+                               "forward_iterations": rf[-1].iterations,
+                               "backward_iterations": rb[-1].iterations,
+                               "rel_diff_x": rel(xk, x_ex), "rel_diff_dL_db": rel(lk, l_ex),
+                               "rel_diff_dL_dvals": rel(gk, g_ex)}
+    P.set_jacobi_sweeps(0)
     P.close()
     dA.close()
     return out
@@ -498,7 +535,7 @@ def profile_case(case, grid, launches):
     'spmv32' (FP32), 'jacobi32' (FP32 IC(0) apply with JACOBI_K Jacobi
     iterations per triangle), 'sweep64' / 'sweep32' (exact IC(0) lower sweep),
     'mixed' (complete mixed solves of the headline configuration, for the
-    launch list)."""
+    launch list), 'batched' (the 512-system batched Jacobi PCG, FP64)."""
     import mtlgpu as M
     A = M.laplacian3d(grid)
     n = A[0]
@@ -524,6 +561,16 @@ def profile_case(case, grid, launches):
             dx.upload(np.zeros(n))
             st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=4000,
                                  mode=M.SOLVE_MIXED, inner_rtol=INNER_RTOL)
+            assert st == M.OK, st
+    elif case == "batched":
+        systems, (nb, rp, ci, v, off) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2,
+                                                      seed=3)
+        dB = M.Csr(ctx, rp, ci, v)
+        P = M.Pc(dB, "diagonal")
+        db, dx = ctx.to_device(M.normal(nb, 3)), ctx.array(nb)
+        for _ in range(launches):
+            dx.upload(np.zeros(nb))
+            st, _ = M.solve_batched(dB, P, off, dx, db, rtol=1e-8, max_iter=5000)
             assert st == M.OK, st
     else:
         prec = M.FP32 if case == "sweep32" else M.FP64
@@ -590,7 +637,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the config-3, batched and differentiable-solve measurements")
     ap.add_argument("--profile-case",
-                    choices=["spmv", "spmv32", "jacobi32", "sweep64", "sweep32", "mixed"])
+                    choices=["spmv", "spmv32", "jacobi32", "sweep64", "sweep32", "mixed",
+                             "batched"])
     ap.add_argument("--sweep-scan", action="store_true",
                     help="per-level cost of the exact sweep on 64^3 .. 192^3 grids")
     ap.add_argument("--grid", type=int, default=64)

@@ -499,8 +499,10 @@ __device__ BatchState solve_system(Team& tm, const BatchArgs& a, const BatchVecs
 // count)) from queue[1] and solves each alone.  No distributed-shared-memory
 // access follows the last cluster barrier of phase 1, so CTAs may leave
 // independently.
+// 4 CTAs per SM: 64 registers a thread, no spills (measured 5 % faster for
+// the FP32-refined and Jacobi-applied IC(0) solves than 3 CTAs at 80).
 template <typename T, int G>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     batch_cluster_kernel(BatchArgs a, BatchVecs<T> V, int refine) {
   __shared__ ClusterSum<3> cs;
   __shared__ int item;
