@@ -299,12 +299,73 @@ class Replicas:
         """Whole-job throughput: all ranks' units over the slowest rank's time."""
         return per_rank_units * self.world / (self.max_over_ranks(ms) / 1e3)
 
+    def gather(self, obj):
+        """Every rank's object, in rank order (all ranks take part)."""
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
+
     def emit(self, line):
         """Only rank 0 prints the JSON line."""
         if self.rank == 0:
             print(json.dumps(line), flush=True)
             return True
         return False
+
+
+def shard_systems(work, world):
+    """Splits independent systems over `world` ranks by estimated work
+    (longest first, each to the least-loaded rank; ties by index), so every
+    rank solves its own share with no exchange between ranks.  Returns each
+    rank's system indices, ascending."""
+    order = sorted(range(len(work)), key=lambda s_: (-work[s_], s_))
+    loads = [0] * world
+    parts = [[] for _ in range(world)]
+    for s_ in order:
+        r = min(range(world), key=lambda k: (loads[k], k))
+        parts[r].append(s_)
+        loads[r] += work[s_]
+    return [sorted(p_) for p_ in parts]
+
+
+def block_diag(systems, idx):
+    """The block-diagonal CSR of systems[i] for i in idx: (n, rp, ci, v, offsets)."""
+    sizes = [systems[i][0] for i in idx]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    rps, cis, vs = [np.zeros(1, np.int32)], [], []
+    e = 0
+    for k, i in enumerate(idx):
+        n_, rp_, ci_, v_ = systems[i]
+        rps.append(rp_[1:] + e)
+        cis.append(ci_ + off[k])
+        vs.append(v_)
+        e += len(ci_)
+    cat = (lambda a, dt: np.concatenate(a).astype(dt) if a else np.zeros(0, dt))
+    return int(off[-1]), cat(rps, np.int32), cat(cis, np.int32), cat(vs, np.float64), off
+
+
+def batched_sharded(M, reps, solve_share, seed=3):
+    """Config 4 across ranks: the 512 systems split by stored entries
+    (shard_systems), each rank solving its share with `solve_share(block
+    diagonal matrix, rhs) -> (ms, iterations per system)`; the job's time is
+    the slowest rank's, the rank results gathered to every rank."""
+    systems, (n, _, _, _, off) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2, seed=seed)
+    b = M.normal(n, seed)
+    parts = shard_systems([len(sy[2]) for sy in systems], reps.world)
+    mine = parts[reps.rank]
+    A = block_diag(systems, mine)
+    rhs = np.concatenate([b[off[i]:off[i + 1]] for i in mine]) if mine else np.zeros(0)
+    ms, its = solve_share(A, rhs)
+    every = reps.gather({"rank": reps.rank, "systems": mine, "iterations": list(its), "ms": ms})
+    slowest = max(e["ms"] for e in every)
+    covered = sorted(s_ for e in every for s_ in e["systems"])
+    return {"systems": len(systems), "ranks": reps.world, "ms": slowest,
+            "systems_per_s": len(systems) / (slowest / 1e3),
+            "per_rank_ms": [e["ms"] for e in every],
+            "per_rank_systems": [len(e["systems"]) for e in every],
+            "all_systems_once": covered == list(range(len(systems)))}
 
 
 def _local_ms(fn, reps, stream):
@@ -887,6 +948,25 @@ def main():
         "clocks": clk,
     }
     A3 = b3 = None
+    if world > 1 and not args.no_extras:
+        # config 4 sharded by systems: no data-path collective
+        def solve_share(Ab, rhs):
+            nb_, rp_, ci_, v_, off_ = Ab
+            dB = M.Csr(ctx, rp_, ci_, v_)
+            Pb = M.Pc(dB, "diagonal")
+            dbb, dxb, dzb = ctx.to_device(rhs), ctx.array(nb_), ctx.to_device(np.zeros(nb_))
+
+            def run():
+                ctx.xpay(dzb, 0.0, dxb)
+                st, res = M.solve_batched(dB, Pb, off_, dxb, dbb, rtol=1e-8, max_iter=5000)
+                assert st == M.OK, st
+                return res
+            run()
+            ms_, rr = timed(run, 2)
+            Pb.close()
+            dB.close()
+            return ms_, [r_.iterations for r_ in rr[-1]]
+        line["batched_sharded"] = batched_sharded(M, reps, solve_share)
     if world == 1 and not args.no_extras:
         A3, b3, line["config3"] = config3_workload(M, ctx, timed, solver, spmv_stats, peak)
         line["batched"] = batched_workload(M, ctx, stream, peak)

@@ -61,3 +61,61 @@ def test_two_gloo_ranks(tmp_path):
     assert outs[0]["printed"] and json.loads(outs[0]["out"])["rank"] == 0
     assert not outs[1]["printed"] and outs[1]["out"] == ""
     assert outs[1]["ran"] == 0
+
+
+def test_shard_systems_and_block_diag(M):
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    systems, (n, rp, ci, v, off) = M.graph_batch(64, 1000, 8192, 8.0, 32.0, 1e-2, seed=3)
+    # the block-diagonal matrix of all systems is the generator's own
+    A = bench.block_diag(systems, list(range(len(systems))))
+    assert A[0] == n and np.array_equal(A[1], rp) and np.array_equal(A[2], ci)
+    assert np.array_equal(A[3], v) and np.array_equal(A[4], off)
+    work = [len(sy[2]) for sy in systems]
+    for world in (1, 2, 3, 8):
+        parts = bench.shard_systems(work, world)
+        assert sorted(s for p in parts for s in p) == list(range(len(systems)))
+        loads = [sum(work[s] for s in p) for p in parts]
+        assert max(loads) - min(loads) <= max(work)          # greedy bound
+
+
+SHARD_WORKER = r'''
+import datetime, json, os, sys
+sys.path.insert(0, {root!r})
+sys.path.insert(0, os.path.join({root!r}, "mtl4-mirror_b200", "python"))
+import torch.distributed as dist
+import bench, mtlgpu as M
+dist.init_process_group("gloo", init_method="tcp://127.0.0.1:{port}", rank=int(sys.argv[1]),
+                        world_size=2, timeout=datetime.timedelta(seconds=60))
+R = bench.Replicas(dist, "cpu")
+def fake_solve(A, rhs):      # stands in for the device solve: work-proportional time
+    n, rp, ci, v, off = A
+    assert len(rhs) == n and len(off) >= 1
+    return len(ci) / 1e6, [1] * (len(off) - 1)
+out = bench.batched_sharded(M, R, fake_solve)
+dist.barrier()
+dist.destroy_process_group()
+print(json.dumps(out))
+'''
+
+
+def test_batched_sharded_two_gloo_ranks(tmp_path):
+    # config 4 split over two ranks: every system solved once, loads balanced,
+    # the job's time the slowest rank's, the same summary on both ranks
+    port = 30500 + (os.getpid() % 1000)
+    src = tmp_path / "shard_worker.py"
+    src.write_text(SHARD_WORKER.format(root=ROOT, port=port))
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1")
+    procs = [subprocess.Popen([sys.executable, str(src), str(r)], stdout=subprocess.PIPE,
+                              stderr=subprocess.PIPE, text=True, env=env) for r in (0, 1)]
+    outs = []
+    for p in procs:
+        o, e = p.communicate(timeout=300)
+        assert p.returncode == 0, e[-2000:]
+        outs.append(json.loads(o.strip().splitlines()[-1]))
+    assert outs[0] == outs[1]
+    o = outs[0]
+    assert o["ranks"] == 2 and o["all_systems_once"] and sum(o["per_rank_systems"]) == 512
+    assert o["ms"] == max(o["per_rank_ms"])
+    assert max(o["per_rank_ms"]) <= 1.01 * min(o["per_rank_ms"])
