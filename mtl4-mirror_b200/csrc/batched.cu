@@ -427,12 +427,12 @@ mtlgpu_status solve_batched_impl(int method, Csr* A, Pc* P, int count, const int
     int cs = A->batch_cs, g = A->batch_g;
     int small = A->batch_small;
     // MTLGPU_BATCH_SHAPE="CTAs,lanes[,small rows]" overrides the tuned shape
-    // (testing)
+    // (testing); lanes 1 selects the CSR-stream SpMV
     if (const char* m = std::getenv("MTLGPU_BATCH_SHAPE")) {
       int c2 = 0, g2 = 0, s2 = -1;
       const int k = std::sscanf(m, "%d,%d,%d", &c2, &g2, &s2);
       if (k >= 2 && (c2 == 1 || c2 == 2 || c2 == 4 || c2 == 8) &&
-          (g2 == 4 || g2 == 8 || g2 == 16 || g2 == 32)) {
+          (g2 == 1 || g2 == 4 || g2 == 8 || g2 == 16 || g2 == 32)) {
         cs = c2, g = g2;
         if (k == 3 && s2 >= 0) small = s2;
       }
@@ -571,7 +571,7 @@ mtlgpu_status batched_autotune_impl(Csr* A, Pc* P, int count, const int32_t* h_o
   float best_ms = 1e30f;
   int best_cs = A->batch_cs, best_g = A->batch_g, best_small = A->batch_small;
   for (int cs : {4, 8})
-    for (int g : {4, 8, 16})
+    for (int g : {1, 4, 8, 16})
       for (int small : {0, 8192, 32768}) {
         cudaMemcpyAsync(x, d_x, sizeof(double) * A->n_rows, cudaMemcpyDeviceToDevice,
                         ctx->stream);

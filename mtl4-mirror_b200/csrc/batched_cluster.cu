@@ -239,6 +239,74 @@ __device__ __forceinline__ void spmv_rows(const int32_t* __restrict__ rp,
   }
 }
 
+// y = A p over rows [lo, hi) in CSR-stream order (G == 1 in the kernel's
+// template): a warp takes 32 consecutive rows and streams their entries in
+// chunks of 32 * KS -- KS coalesced loads of column indices and of values per
+// lane, then KS gathers of p, all in flight at once -- stages the products in
+// its shared-memory slice, and lane l adds the products of row r0 + l that
+// fall in the chunk, in column order.  A warp keeps 2 KS coalesced loads in
+// flight instead of a lane group's few strided ones: the large systems of a
+// batch, solved by one cluster each, are bound by the bytes a CTA has in
+// flight.
+template <typename T>
+__device__ __forceinline__ void spmv_rows_stream(const int32_t* __restrict__ rp,
+                                                 const int32_t* __restrict__ ci,
+                                                 const T* __restrict__ val, const T* p, T* y,
+                                                 int lo, int hi, double& pq, bool dot) {
+  constexpr int KS = 8;
+  constexpr int W = kThreads / 32;
+  __shared__ T sh[W][32 * KS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T* pw = sh[warp];
+  for (int r0 = lo + warp * 32; r0 < hi; r0 += W * 32) {
+    const int nr = min(32, hi - r0);
+    const int row = r0 + lane;
+    int rb = 0, re = 0;
+    if (lane < nr) {
+      rb = rp[row];
+      re = rp[row + 1];
+    }
+    const int e0 = __shfl_sync(0xffffffffu, rb, 0);
+    const int e1 = __shfl_sync(0xffffffffu, re, nr - 1);
+    T s = T(0);
+    for (int c0 = e0; c0 < e1; c0 += 32 * KS) {
+      int c[KS];
+      T v[KS];
+#pragma unroll
+      for (int k = 0; k < KS; k++) {
+        const int j = c0 + k * 32 + lane;
+        c[k] = j < e1 ? ci[j] : 0;
+        v[k] = j < e1 ? val[j] : T(0);
+      }
+#pragma unroll
+      for (int k = 0; k < KS; k++) {
+        const int j = c0 + k * 32 + lane;
+        if (j < e1) pw[k * 32 + lane] = v[k] * __ldcg(p + c[k]);
+      }
+      __syncwarp();
+      const int a = max(rb, c0), b = min(re, c0 + 32 * KS);
+      for (int j = a; j < b; j++) s += pw[j - c0];
+      __syncwarp();
+    }
+    if (lane < nr) {
+      y[row] = s;
+      if (dot) pq += (double)__ldcg(p + row) * (double)s;
+    }
+  }
+}
+
+// The SpMV of the kernel's shape: CSR-stream (G == 1) or G lanes per row.
+template <typename T, int G>
+__device__ __forceinline__ void spmv_team_rows(const int32_t* __restrict__ rp,
+                                               const int32_t* __restrict__ ci,
+                                               const T* __restrict__ val, const T* p, T* y,
+                                               int lo, int hi, double& pq, bool dot) {
+  if constexpr (G == 1)
+    spmv_rows_stream<T>(rp, ci, val, p, y, lo, hi, pq, dot);
+  else
+    spmv_rows<T, G>(rp, ci, val, p, y, lo, hi, pq, dot);
+}
+
 // One Jacobi pass of a factor over rows [lo, hi): out = v - Nt in, times the
 // stored diagonal when scale (jacobi_sweep.cu).
 template <typename T>
@@ -333,7 +401,7 @@ __device__ int pcg_system(Team& tm, const BatchArgs& a,
   const T* A = vals<T>(a);
   double pq_dummy = 0;
   if (direct) {  // r = b - A x (x is the caller's initial guess)
-    spmv_rows<T, G>(a.rp, a.ci, A, x, V.q, lo, hi, pq_dummy, false);
+    spmv_team_rows<T, G>(a.rp, a.ci, A, x, V.q, lo, hi, pq_dummy, false);
     __syncthreads();  // rows were written by their lane groups, read by thread
     for (int i = lo + threadIdx.x; i < hi; i += kThreads) V.r[i] = (T)a.b[i] - V.q[i];
   }
@@ -390,7 +458,7 @@ __device__ int pcg_system(Team& tm, const BatchArgs& a,
     }
     tm.sync();  // p complete before the SpMV gathers it
     double s2[3] = {0, 0, 0};
-    spmv_rows<T, G>(a.rp, a.ci, A, V.p, V.q, lo, hi, s2[0], true);
+    spmv_team_rows<T, G>(a.rp, a.ci, A, V.p, V.q, lo, hi, s2[0], true);
     tm.sum(s2);
     const T alpha = (T)(rho / s2[0]);
     double s3[3] = {0, 0, 0};
@@ -449,7 +517,7 @@ __device__ BatchState solve_system(Team& tm, const BatchArgs& a, const BatchVecs
     int total = 0, outer = 0;
     while (true) {
       double pq_dummy = 0;
-      spmv_rows<double, G>(a.rp, a.ci, A64, a.x, a.r64, lo, hi, pq_dummy, false);
+      spmv_team_rows<double, G>(a.rp, a.ci, A64, a.x, a.r64, lo, hi, pq_dummy, false);
       __syncthreads();  // rows were written by their lane groups, read by thread
       double s0[3] = {0, 0, 0};
       for (int i = lo + threadIdx.x; i < hi; i += kThreads) {
@@ -592,6 +660,7 @@ template <typename T>
 cudaError_t launch_g(cudaStream_t st, int g, int cs, int clusters, const BatchArgs& a,
                      const BatchVecs<T>& V, int refine) {
   switch (g) {
+    case 1: return launch_cluster<T, 1>(st, cs, clusters, a, V, refine);
     case 4: return launch_cluster<T, 4>(st, cs, clusters, a, V, refine);
     case 16: return launch_cluster<T, 16>(st, cs, clusters, a, V, refine);
     case 32: return launch_cluster<T, 32>(st, cs, clusters, a, V, refine);
@@ -602,6 +671,7 @@ cudaError_t launch_g(cudaStream_t st, int g, int cs, int clusters, const BatchAr
 template <typename T>
 int clusters_for(int g, int cs) {
   switch (g) {
+    case 1: return max_clusters<T, 1>(cs);
     case 4: return max_clusters<T, 4>(cs);
     case 16: return max_clusters<T, 16>(cs);
     case 32: return max_clusters<T, 32>(cs);

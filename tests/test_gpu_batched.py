@@ -97,7 +97,7 @@ def _restore(old):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", ["1,8", "2,4", "4,16", "8,32", "8,8,0", "4,8,1500",
-                                   "8,16,100000"])
+                                   "8,16,100000", "4,1", "8,1,0", "2,1,1500", "1,1"])
 def test_batched_cluster_shapes_match_each_system(M, ctx, restate, shape):
     # every (CTAs per system, lanes per row, rows below which one CTA solves
     # a system) shape of the persistent launch gives each system the
