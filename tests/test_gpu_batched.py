@@ -158,7 +158,8 @@ def test_batched_autotune(M, ctx, restate):
     dx, db = ctx.to_device(x0), ctx.to_device(b)
     choice = M.batched_autotune(dA, P, off, dx, db, rtol=1e-8, max_iter=2000)
     assert choice // 1000 in (0, 8192, 32768)
-    assert (choice % 1000) // 100 in (4, 8) and choice % 100 in (4, 8, 16)
+    # lanes per row 1: the CSR-stream SpMV shape
+    assert (choice % 1000) // 100 in (4, 8) and choice % 100 in (1, 4, 8, 16)
     assert np.array_equal(dx.download(), x0)      # the caller's x is not touched
     dx.upload(np.zeros(n))
     st, res = M.solve_batched(dA, P, off, dx, db, rtol=1e-8, max_iter=2000)
