@@ -617,7 +617,8 @@ def profile_case(case, grid, launches):
     'spmv32' (FP32), 'jacobi32' (FP32 IC(0) apply with JACOBI_K Jacobi
     iterations per triangle), 'sweep64' / 'sweep32' (exact IC(0) lower sweep),
     'mixed' (complete mixed solves of the headline configuration, for the
-    launch list), 'batched' (the 512-system batched Jacobi PCG, FP64)."""
+    launch list), 'batched' (the 512-system batched Jacobi PCG, FP64),
+    'assemble' (device assembly of the N^3 Laplacian from shuffled triplets)."""
     import mtlgpu as M
     A = M.laplacian3d(grid)
     n = A[0]
@@ -644,6 +645,12 @@ def profile_case(case, grid, launches):
             st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=4000,
                                  mode=M.SOLVE_MIXED, inner_rtol=INNER_RTOL)
             assert st == M.OK, st
+    elif case == "assemble":
+        Af, r, c, v = assembly_triplets(M, grid)
+        nf = Af[0]
+        dr, dc, dv = ctx.to_device(r), ctx.to_device(c), ctx.to_device(v)
+        for _ in range(launches):
+            M.Csr.assemble(ctx, nf, nf, dr, dc, dv).close()
     elif case == "batched":
         systems, (nb, rp, ci, v, off) = M.graph_batch(512, 1000, 65536, 8.0, 32.0, 1e-2,
                                                       seed=3)
@@ -720,7 +727,7 @@ def main():
                     help="skip the config-3, batched and differentiable-solve measurements")
     ap.add_argument("--profile-case",
                     choices=["spmv", "spmv32", "jacobi32", "sweep64", "sweep32", "mixed",
-                             "batched"])
+                             "batched", "assemble"])
     ap.add_argument("--sweep-scan", action="store_true",
                     help="per-level cost of the exact sweep on 64^3 .. 192^3 grids")
     ap.add_argument("--grid", type=int, default=64)
