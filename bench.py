@@ -119,6 +119,17 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def sell_index_bytes(rp, ci):
+    """Bytes of column index per stored entry in the library's SELL-32 copies:
+    2 (16-bit offsets from the row) when every entry lies within 32,767 of its
+    row and MTLGPU_SELL_INDEX is not 32, else 4.  Factors of IC(0)/ILU(0) have
+    a subset of the matrix's pattern, so the matrix decides for them too."""
+    if os.environ.get("MTLGPU_SELL_INDEX", "") == "32" or len(ci) == 0:
+        return 4
+    rows = np.repeat(np.arange(len(rp) - 1, dtype=np.int64), np.diff(rp))
+    return 2 if int(np.abs(ci.astype(np.int64) - rows).max()) <= 32767 else 4
+
+
 def problem(M):
     A = M.laplacian3d(N_GRID)
     xt = M.uniform(A[0], 1)
@@ -859,29 +870,37 @@ def main():
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs) / reps_
 
-    def spmv_stats(dA_, n_, nnz_, reps_=100):
+    def spmv_stats(dA_, n_, nnz_, ib_, reps_=100):
+        # algorithmic bytes: 8-byte value + ib_-byte index per entry, the
+        # slice offsets, x once and y once
         dxs, dys = ctx.to_device(M.uniform(n_, 5)), ctx.array(n_)
         for _ in range(5):
             dA_.spmv(dxs, dys)
         ms, _ = timed(lambda: dA_.spmv(dxs, dys), reps_)
         ms_cold = cold_ms(lambda: dA_.spmv(dxs, dys), 30)
-        byt = nnz_ * 12 + 4 * (n_ + 1) + 2 * n_ * 8
+        byt = nnz_ * (8 + ib_) + 4 * (n_ // 32 + 1) + 2 * n_ * 8
         return {"ms": ms, "GBps": byt / ms / 1e6, "hbm_frac": byt / ms / 1e6 / peak,
-                "bytes": byt, "peak_kind": peak_kind,
+                "bytes": byt, "index_bytes": ib_, "peak_kind": peak_kind,
                 "back_to_back": "mean of %d products back to back" % reps_,
                 "cold": {"ms": ms_cold, "GBps": byt / ms_cold / 1e6,
                          "hbm_frac": byt / ms_cold / 1e6 / peak,
                          "how": "L2 flushed before each product, per-launch CUDA events"}}
 
-    spmv = spmv_stats(dA, n, nnz)
+    ib = sell_index_bytes(A[1], A[2])
+    spmv = spmv_stats(dA, n, nnz, ib)
 
-    # The mixed solve's kernels, timed alone on the same data (FP32): the
-    # Jacobi passes of the IC(0) apply and the FP32 SpMV.  Algorithmic bytes:
-    # a pass reads the factor's off-diagonal entries (4-byte value + 4-byte
-    # index), v, D and the previous iterate once and writes one vector; the
-    # SpMV as above with 4-byte values and vectors.
+    # The mixed solve's kernels, timed alone on the same data (FP32).  Per
+    # inner iteration the solve runs three: the direction product
+    # (p = z + beta p, q = A p, p.q), the first L pass fused with the x / r
+    # update, and the U pass with r.z; the first and the last are timed here
+    # (the fused L pass has no entry point of its own; its share is in the
+    # launch-list profile).  Algorithmic bytes: the product reads A's entries
+    # (4-byte value + 4-byte index), the slice offsets, z and p once and
+    # writes p and q; a Jacobi pass reads the factor's off-diagonal entries
+    # (4-byte value + ib-byte index), v, D and the previous iterate once and
+    # writes one vector.  The plain FP32 SpMV is timed for the record.
     nnz_off = P32.factor_info(M.LOWER)[0] - n
-    bytes_pass = nnz_off * 8 + 4 * (n // 32 + 1) + 4 * n * 4
+    bytes_pass = nnz_off * (4 + ib) + 4 * (n // 32 + 1) + 4 * n * 4
     r32 = ctx.to_device(np.ones(n, np.float32))
     z32 = ctx.array(n, np.float32)
     for _ in range(3):
@@ -894,7 +913,18 @@ def main():
     for _ in range(5):
         dA.spmv_f32(x32, y32)
     ms_spmv32, _ = timed(lambda: dA.spmv_f32(x32, y32), 100)
-    bytes_spmv32 = nnz * 8 + 4 * (n + 1) + 2 * n * 4
+    bytes_spmv32 = nnz * 8 + 4 * (n // 32 + 1) + 2 * n * 4   # 4-byte indices in FP32
+    p32, po32, q32, dpq = (ctx.to_device(M.uniform(n, 6).astype(np.float32)),
+                           ctx.array(n, np.float32), ctx.array(n, np.float32), ctx.array(1))
+
+    def direction():
+        dA.cg_direction_product(M.FP32, x32, 0.5, p32, po32, q32, dpq)
+
+    for _ in range(5):
+        direction()
+    ms_dir32, _ = timed(direction, 100)
+    ms_dir32_cold = cold_ms(direction, 30)
+    bytes_dir32 = nnz * 8 + 4 * (n // 32 + 1) + 4 * n * 4
     traffic = read_traffic()
 
     # exact sweeps (the FP64 path's dominant kernel), for the record
@@ -921,10 +951,11 @@ def main():
     ms_e2e = max_over_ranks(ms_e2e)
 
     dominant = {
-        "jacobi_pass_kernel<float> (IC(0) apply, 1 Jacobi pass)": (ms_pass, bytes_pass,
-                                                                    2 * JACOBI_K,
-                                                                    "jacobi_pass_f32"),
-        "spmv_sell<float,8> (q = A p, FP32)": (ms_spmv32, bytes_spmv32, 1, "spmv_sell_f32"),
+        "jacobi_pass_kernel<float> (IC(0) U pass, r.z fused)": (ms_pass, bytes_pass,
+                                                                 2 * JACOBI_K - 1,
+                                                                 "jacobi_pass_f32"),
+        "cg_pspmv_kernel<float> (p = z + beta p, q = A p, p.q)": (ms_dir32, bytes_dir32, 1,
+                                                                   "cg_pspmv_f32"),
     }
     dom = max(dominant, key=lambda k: dominant[k][0] * dominant[k][2])
     d_ms, d_bytes, _, d_key = dominant[dom]
@@ -941,7 +972,9 @@ def main():
         "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": n, "nnz": nnz, "index": "int32",
+        "config": {"workload": WORKLOAD, "n": n, "nnz": nnz,
+                   "index": "int32 CSR; SELL-32 column indices: %d bytes in the FP64 "
+                            "SpMV and the Jacobi passes, 4 in the FP32 SpMV" % ib,
                    "jacobi_iterations_per_triangle": JACOBI_K, "inner_rtol": INNER_RTOL,
                    "l2": "inputs larger than L2 (matrix 175 MB + factors 2 x 100 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -960,9 +993,13 @@ def main():
                      "peak": peak, "unit": "GB/s", "frac": d_bytes / d_ms / 1e6 / peak,
                      "traffic": traffic.get(d_key), "algorithmic_bytes": d_bytes,
                      "ms": d_ms, "peak_kind": peak_kind},
-        "mixed_kernels": {"jacobi_pass_f32": {"ms": ms_pass, "GBps": bytes_pass / ms_pass / 1e6,
+        "mixed_kernels": {"cg_pspmv_f32": {"ms": ms_dir32, "GBps": bytes_dir32 / ms_dir32 / 1e6,
+                                           "bytes": bytes_dir32, "launches_per_iteration": 1,
+                                           "cold_ms": ms_dir32_cold,
+                                           "cold_GBps": bytes_dir32 / ms_dir32_cold / 1e6},
+                          "jacobi_pass_f32": {"ms": ms_pass, "GBps": bytes_pass / ms_pass / 1e6,
                                               "bytes": bytes_pass,
-                                              "launches_per_iteration": 2 * JACOBI_K,
+                                              "launches_per_iteration": 2 * JACOBI_K - 1,
                                               "cold_ms": ms_pass_cold,
                                               "cold_GBps": bytes_pass / ms_pass_cold / 1e6},
                           "spmv_f32": {"ms": ms_spmv32, "GBps": bytes_spmv32 / ms_spmv32 / 1e6,
@@ -1041,7 +1078,7 @@ def config3_workload(M, ctx, timed, solver, spmv_stats, peak):
                           "mixed_outer": rmx[-1].outer_iterations},
            "true_rel_residual": float(np.linalg.norm(b - M.csr_mult(A, x)) / np.linalg.norm(b)),
            "jacobi_iterations_per_triangle": JACOBI_K,
-           "spmv": spmv_stats(dA, n, nnz)}
+           "spmv": spmv_stats(dA, n, nnz, sell_index_bytes(A[1], A[2]))}
     P32.close()
     P64.close()
     dA.close()

@@ -259,6 +259,19 @@ mtlgpu_status mtlgpu_spmv_f32(mtlgpu_csr* A, const float* d_x, float* d_y);
 /* y = A^T x (trans(A) * x; transposed_sparse_matrix_vector_product_test.cpp:32). */
 mtlgpu_status mtlgpu_spmv_transposed(mtlgpu_csr* A, const double* d_x, double* d_y);
 
+/* CG's search-direction step in one kernel: p_out = z + beta * p (p_out = z
+ * when d_p is NULL), q = A * p_out, *d_pq = dot(p_out, q) (device double).
+ * itl::cg runs it as `p = z + beta * p; q = A * p; alpha = rho / dot(p, q)`
+ * (itl/krylov/cg.hpp:99-104, the product and the dot fused as in
+ * fused_expr.hpp:57-77); it is the product kernel of the device CG with
+ * Jacobi-applied factors.  prec MTLGPU_FP32 (float vectors, A's values
+ * rounded to float) or MTLGPU_FP64.  p_out must differ from z and p.  Needs
+ * the SELL-32 layout (MTLGPU_NOT_SUPPORTED otherwise).  Asynchronous on the
+ * context's stream. */
+mtlgpu_status mtlgpu_cg_direction_product(mtlgpu_csr* A, int prec, const void* d_z, double beta,
+                                          const void* d_p, void* d_p_out, void* d_q,
+                                          double* d_pq);
+
 /* ---- BLAS-1 (mtl/operation/dot.hpp:226-232, two_norm.hpp:33-57,
  *      unary_dot.hpp:29-65, vector/vec_vec_aop_expr.hpp:60-152).
  *      Results are written to host scalars. */

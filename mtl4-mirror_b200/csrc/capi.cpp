@@ -413,6 +413,27 @@ mtlgpu_status mtlgpu_spmv(mtlgpu_csr* A, const double* x, double* y, double alph
   return MTLGPU_OK;
 }
 
+mtlgpu_status mtlgpu_cg_direction_product(mtlgpu_csr* A, int prec, const void* d_z, double beta,
+                                          const void* d_p, void* d_p_out, void* d_q,
+                                          double* d_pq) {
+  if (!A || (prec != MTLGPU_FP32 && prec != MTLGPU_FP64)) return MTLGPU_INVALID_ARG;
+  if (A->n_rows != A->n_cols) return MTLGPU_NOT_SQUARE;
+  if (A->n_rows && (!d_z || !d_p_out || !d_q || !d_pq || d_p_out == d_z || d_p_out == d_p ||
+                    d_q == d_z || d_q == d_p || d_q == d_p_out))
+    return MTLGPU_INVALID_ARG;
+  if (prec == MTLGPU_FP32) {
+    MTLGPU_TRY(csr_ensure_fp32(A));
+    return cg_direction_product<float>(A, static_cast<const float*>(d_z), beta,
+                                       static_cast<const float*>(d_p),
+                                       static_cast<float*>(d_p_out), static_cast<float*>(d_q),
+                                       d_pq);
+  }
+  return cg_direction_product<double>(A, static_cast<const double*>(d_z), beta,
+                                      static_cast<const double*>(d_p),
+                                      static_cast<double*>(d_p_out), static_cast<double*>(d_q),
+                                      d_pq);
+}
+
 mtlgpu_status mtlgpu_spmv_f32(mtlgpu_csr* A, const float* x, float* y) {
   if (!A || (A->n_rows && (!x || !y)) || x == y) return MTLGPU_INVALID_ARG;
   MTLGPU_TRY(csr_ensure_fp32(A));

@@ -64,6 +64,10 @@ struct Sell {
   bool col_scaled = false;         // entry (r, c) stored as a_rc * dinv[c]
   int32_t* d_slice_ptr = nullptr;  // n_slices + 1 entry offsets (multiples of 32)
   int32_t* d_col = nullptr;
+  // column - row as 16 bits (padding: -32768), built when every entry lies
+  // within 32,767 of its row (banded / stencil patterns): the streaming
+  // kernels then read 2 bytes of index per entry instead of 4
+  int16_t* d_dcol = nullptr;
   double* d_val = nullptr;
   float* d_val32 = nullptr;
   double* d_dinv = nullptr;
@@ -277,7 +281,24 @@ template <typename T>
 mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T* scratch,
                            const int* skip, const T* dot_with = nullptr,
                            double* dot_out = nullptr);
+template <typename T>
+mtlgpu_status jacobi_solve_from(Ctx* ctx, const Sell& J, int k, int first, const T* v, T* out,
+                                T* scratch, const int* skip, const T* dot_with = nullptr,
+                                double* dot_out = nullptr);
 mtlgpu_status pc_set_jacobi(Pc* P, int iters);
+
+// Preconditioned CG with Jacobi-applied IC(0)/ILU(0) in three kernels per
+// iteration (cg_fused.cu).  `st` is the solve's device SolverState.
+struct SolverState;
+bool cg_fused_eligible(Csr* A, Pc* P, int prec);
+template <typename T>
+mtlgpu_status cg_fused_prologue(Csr* A, Pc* P, SolverState* st, const T* r, T* z, T* p, T* q);
+template <typename T>
+mtlgpu_status cg_direction_product(Csr* A, const T* z, double beta, const T* p, T* p_next, T* q,
+                                   double* d_pq);
+template <typename T>
+mtlgpu_status cg_fused_iteration(Csr* A, Pc* P, SolverState* st, T* x, const T* r, T* r_next,
+                                 const T* p, T* p_next, T* z, T* q);
 
 // Analysis (analysis.cu)
 mtlgpu_status build_sweep_plan(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_ci,

@@ -61,10 +61,12 @@ struct PassDot {
 // row are taken in chunks of C: all C column indices and values are loaded
 // (last-use hint), then all C gathers issued, so a row costs one DRAM and
 // one L2 round trip per chunk.
-template <typename T, bool SCALE, bool DOT, int C>
+// With D16 the column indices are 16-bit offsets from the row (Sell::d_dcol).
+template <typename T, bool SCALE, bool DOT, int C, bool D16>
 __global__ void __launch_bounds__(kBlock, (C == 4 && sizeof(T) == 4) ? 8 : 6)
     jacobi_pass_kernel(int n, const int32_t* __restrict__ slice_ptr,
-                       const int32_t* __restrict__ col, const T* __restrict__ val,
+                       const int32_t* __restrict__ col, const int16_t* __restrict__ dcol,
+                       const T* __restrict__ val,
                        const T* __restrict__ dinv, const T* __restrict__ v,
                        const T* __restrict__ in, T* __restrict__ out, const int* skip,
                        PassDot dot) {
@@ -79,6 +81,7 @@ __global__ void __launch_bounds__(kBlock, (C == 4 && sizeof(T) == 4) ? 8 : 6)
     const T vr = __ldg(v + r);
     const T dr = SCALE ? __ldg(dinv + r) : T(1);
     const int32_t* cp = col + base + lane;
+    const int16_t* dp = dcol + base + lane;
     const T* vp = val + base + lane;
     T acc = T(0);
     for (int k0 = 0; k0 < width; k0 += C) {
@@ -87,7 +90,12 @@ __global__ void __launch_bounds__(kBlock, (C == 4 && sizeof(T) == 4) ? 8 : 6)
 #pragma unroll
       for (int u = 0; u < C; u++) {
         const bool inr = k0 + u < width;
-        c[u] = inr ? __ldlu(cp + 32 * (k0 + u)) : -1;
+        if (D16) {
+          const int d = inr ? (int)__ldlu(dp + 32 * (k0 + u)) : -32768;
+          c[u] = d == -32768 ? -1 : (int)r + d;
+        } else {
+          c[u] = inr ? __ldlu(cp + 32 * (k0 + u)) : -1;
+        }
         a[u] = inr ? __ldlu(vp + 32 * (k0 + u)) : T(0);
       }
 #pragma unroll
@@ -128,13 +136,22 @@ struct JVals<float> {
 template <typename T, bool SCALE>
 void launch2(int grid, cudaStream_t st, const Sell& J, const T* val, const T* dinv, const T* v,
              const T* in, T* out, const int* skip, const PassDot& dot) {
-#define MTLGPU_JP(DOT, C)                                                               \
-  jacobi_pass_kernel<T, SCALE, DOT, C><<<grid, kBlock, 0, st>>>(                        \
-      J.n, J.d_slice_ptr, J.d_col, val, dinv, v, in, out, skip, dot)
+#define MTLGPU_JP(DOT, C, D16)                                                          \
+  jacobi_pass_kernel<T, SCALE, DOT, C, D16><<<grid, kBlock, 0, st>>>(                   \
+      J.n, J.d_slice_ptr, J.d_col, J.d_dcol, val, dinv, v, in, out, skip, dot)
+  const bool d16 = J.d_dcol != nullptr;
   if (J.max_width <= 4) {
-    if (dot.out) MTLGPU_JP(true, 4); else MTLGPU_JP(false, 4);
+    if (dot.out) {
+      if (d16) MTLGPU_JP(true, 4, true); else MTLGPU_JP(true, 4, false);
+    } else {
+      if (d16) MTLGPU_JP(false, 4, true); else MTLGPU_JP(false, 4, false);
+    }
   } else {
-    if (dot.out) MTLGPU_JP(true, 8); else MTLGPU_JP(false, 8);
+    if (dot.out) {
+      if (d16) MTLGPU_JP(true, 8, true); else MTLGPU_JP(true, 8, false);
+    } else {
+      if (d16) MTLGPU_JP(false, 8, true); else MTLGPU_JP(false, 8, false);
+    }
   }
 #undef MTLGPU_JP
 }
@@ -162,12 +179,16 @@ mtlgpu_status pass_launch(Ctx* ctx, const Sell& J, bool scale, const T* v, const
 // so that the last one writes out.
 // With dot_with non-null the last pass also writes dot_with . out to
 // *dot_out (reduction slot `counter_index` of the context).
+//
+// jacobi_solve_from runs passes first..k-1 only, after pass 0 (first = 1)
+// was made elsewhere (the fused CG kernel, cg_fused.cu) into the buffer that
+// jacobi_solve would have used: out when k is odd, else scratch.
 template <typename T>
-mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T* scratch,
-                           const int* skip, const T* dot_with, double* dot_out) {
+mtlgpu_status jacobi_solve_from(Ctx* ctx, const Sell& J, int k, int first, const T* v, T* out,
+                                T* scratch, const int* skip, const T* dot_with, double* dot_out) {
   if (J.n == 0) return MTLGPU_OK;
-  const T* prev = v;  // u_0 = v
-  for (int i = 0; i < k; i++) {
+  const T* prev = first == 0 ? v : (((k - first) % 2 == 0) ? out : scratch);  // u_0 = v
+  for (int i = first; i < k; i++) {
     T* dst = ((k - 1 - i) % 2 == 0) ? out : scratch;
     PassDot dot;
     if (i == k - 1 && dot_with) {
@@ -182,6 +203,17 @@ mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T
   return MTLGPU_OK;
 }
 
+template <typename T>
+mtlgpu_status jacobi_solve(Ctx* ctx, const Sell& J, int k, const T* v, T* out, T* scratch,
+                           const int* skip, const T* dot_with, double* dot_out) {
+  return jacobi_solve_from<T>(ctx, J, k, 0, v, out, scratch, skip, dot_with, dot_out);
+}
+
+template mtlgpu_status jacobi_solve_from<double>(Ctx*, const Sell&, int, int, const double*,
+                                                 double*, double*, const int*, const double*,
+                                                 double*);
+template mtlgpu_status jacobi_solve_from<float>(Ctx*, const Sell&, int, int, const float*, float*,
+                                                float*, const int*, const float*, double*);
 template mtlgpu_status jacobi_solve<double>(Ctx*, const Sell&, int, const double*, double*,
                                             double*, const int*, const double*, double*);
 template mtlgpu_status jacobi_solve<float>(Ctx*, const Sell&, int, const float*, float*,

@@ -28,31 +28,16 @@
 
 #include "device.cuh"
 #include "internal.h"
+#include "solver_state.cuh"
 
 namespace mtlgpu {
 
 using namespace dev;
 
 constexpr int kGraphIters = 8;
-
-struct SolverState {
-  int done;       // nonzero: every kernel returns immediately
-  int skip2;      // BiCGSTAB: second half of the iteration skipped
-  int half_exit;  // BiCGSTAB: finished on ||s||
-  int error;      // basic_iteration error code (0, 1)
-  int status;     // mtlgpu_status (BREAKDOWN, ...)
-  int iter;       // basic_iteration::i
-  int max_iter;
-  int hist_len;
-  int hist_cap;
-  int pad;
-  double tol;     // rtol * norm_r0
-  double atol;
-  double norm_r0;
-  double resid;
-  double rho, rho_1, rr, alpha_1, gamma, omega, ts, tt, ss;
-  double* history;
-};
+// The fused CG recording alternates two r and two p buffers by iteration
+// parity; an even count per graph keeps the parity across graph launches.
+static_assert(kGraphIters % 2 == 0, "graphs hold an even number of iterations");
 
 namespace {
 
@@ -62,21 +47,6 @@ int vec_grid(Ctx* ctx, long long n) {
   long long need = (n + kBlock - 1) / kBlock;
   long long cap = (long long)ctx->num_sms * 8;
   return (int)std::max(1ll, std::min(need, cap));
-}
-
-// basic_iteration::finished(r) (basic_iteration.hpp:60-65 with converged()
-// 85-93 and check_max() 43-48).  Called by one thread.
-__device__ bool iter_finished(SolverState* st, double r) {
-  if (st->history && st->hist_len < st->hist_cap) st->history[st->hist_len] = r;
-  st->hist_len++;
-  st->resid = r;
-  bool conv = st->norm_r0 == 0.0 ? (r <= st->atol) : (r <= st->tol || r <= st->atol);
-  if (conv) return true;
-  if (st->iter >= st->max_iter) {
-    st->error = 1;
-    return true;
-  }
-  return false;
 }
 
 template <typename T>
@@ -489,6 +459,9 @@ struct Workspace {
   int n = 0;
   T *x = nullptr, *b = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr,
     *rt = nullptr, *phat = nullptr, *s = nullptr, *shat = nullptr, *t = nullptr, *v = nullptr;
+  // fused CG (cg_fused.cu): second r and p buffers, odd iterations write them
+  bool fused = false;
+  T *r2 = nullptr, *p2 = nullptr;
   SolverState* st = nullptr;   // device
   SolverState* h_st = nullptr; // pinned host mirror
   double* history = nullptr;
@@ -531,11 +504,17 @@ mtlgpu_status apply_pc(Workspace<T>* W, const T* r, T* z, const int* skip, bool 
   return MTLGPU_OK;
 }
 
-// Kernels of one CG iteration.
+// Kernels of one CG iteration (k: its index inside the graph).
 template <typename T>
-mtlgpu_status record_cg_iteration(Workspace<T>* W) {
+mtlgpu_status record_cg_iteration(Workspace<T>* W, int k) {
   Csr* A = W->A;
   Ctx* ctx = A->ctx;
+  if (W->fused) {
+    const bool even = k % 2 == 0;
+    return cg_fused_iteration<T>(A, W->P, W->st, W->x, even ? W->r : W->r2,
+                                 even ? W->r2 : W->r, even ? W->p : W->p2, even ? W->p2 : W->p,
+                                 W->z, W->q);
+  }
   const int n = W->n;
   const int grid = vec_grid(ctx, n);
   const bool ident = is_identity(W->P);
@@ -617,7 +596,7 @@ mtlgpu_status build_graph(Workspace<T>* W) {
   MTLGPU_TRY_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   mtlgpu_status s = MTLGPU_OK;
   for (int k = 0; k < kGraphIters && s == MTLGPU_OK; k++)
-    s = W->method == MTLGPU_CG ? record_cg_iteration<T>(W) : record_bicgstab_iteration<T>(W);
+    s = W->method == MTLGPU_CG ? record_cg_iteration<T>(W, k) : record_bicgstab_iteration<T>(W);
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
   ctx->launches = launches_before;
   if (s != MTLGPU_OK) {
@@ -651,6 +630,10 @@ mtlgpu_status alloc_workspace(Workspace<T>* W) {
   MTLGPU_TRY(dalloc(ctx, &W->p, n));
   MTLGPU_TRY(dalloc(ctx, &W->q, n));
   if (!is_identity(W->P) || W->method == MTLGPU_BICGSTAB) MTLGPU_TRY(dalloc(ctx, &W->z, n));
+  if (W->fused) {
+    MTLGPU_TRY(dalloc(ctx, &W->r2, n));
+    MTLGPU_TRY(dalloc(ctx, &W->p2, n));
+  }
   if (W->method == MTLGPU_BICGSTAB) {
     MTLGPU_TRY(dalloc(ctx, &W->rt, n));
     MTLGPU_TRY(dalloc(ctx, &W->phat, n));
@@ -672,7 +655,7 @@ void release_workspace(Workspace<T>* W) {
   Ctx* ctx = W->A->ctx;
   if (W->exec) cudaGraphExecDestroy(W->exec);
   T** bufs[] = {&W->x, &W->b, &W->r, &W->z, &W->p, &W->q, &W->rt, &W->phat, &W->s, &W->shat,
-                &W->t, &W->v};
+                &W->t, &W->v, &W->r2, &W->p2};
   for (T** b : bufs) dfree(ctx, *b);
   dfree(ctx, W->st);
   dfree(ctx, W->history);
@@ -705,6 +688,7 @@ mtlgpu_status get_workspace(Csr* A, Pc* P, int method, Workspace<T>** out) {
   W->P = P;
   W->method = method;
   W->n = A->n_rows;
+  W->fused = method == MTLGPU_CG && cg_fused_eligible(A, P, prec);
   mtlgpu_status s = alloc_workspace<T>(W);
   if (s != MTLGPU_OK) {
     release_workspace<T>(W);
@@ -820,6 +804,8 @@ mtlgpu_status device_solve(Workspace<T>* W, const mtlgpu_iter_params* prm, doubl
     fill2_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, pc_tmp<T>(W->P), second);
     ctx->launches++;
   }
+  // the fused recording starts inside the first iteration (z, rho, p, q)
+  if (W->fused) MTLGPU_TRY(cg_fused_prologue<T>(A, W->P, W->st, W->r, W->z, W->p, W->q));
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   int interrupted = 0;
   MTLGPU_TRY(run_iterations<T>(W, prm->h_interrupt, &interrupted));

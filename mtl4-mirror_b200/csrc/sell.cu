@@ -15,6 +15,7 @@
 // Jacobi-iteration triangular solves (jacobi_sweep.cu, off-diagonal part with
 // the diagonal kept apart).
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "device.cuh"
@@ -108,7 +109,63 @@ __global__ void slice_fill_kernel(int n, const int32_t* __restrict__ rp,
   }
 }
 
+// Largest |column - row| over the stored entries (padding skipped).
+__global__ void delta_max_kernel(int n, const int32_t* __restrict__ slice_ptr,
+                                 const int32_t* __restrict__ col, int* __restrict__ out) {
+  int m = 0;
+  for (long long r = gtid(); r < n; r += gstride()) {
+    const long long s = r >> 5;
+    const int lane = (int)(r & 31);
+    const int base = slice_ptr[s], width = (slice_ptr[s + 1] - base) >> 5;
+    for (int k = 0; k < width; k++) {
+      const int c = col[base + 32 * k + lane];
+      if (c >= 0) m = max(m, abs(c - (int)r));
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// 16-bit column deltas: column - row, padding -32768.
+__global__ void dcol_fill_kernel(int n, const int32_t* __restrict__ slice_ptr,
+                                 const int32_t* __restrict__ col, int16_t* __restrict__ dcol) {
+  for (long long r = gtid(); r < n; r += gstride()) {
+    const long long s = r >> 5;
+    const int lane = (int)(r & 31);
+    const int base = slice_ptr[s], width = (slice_ptr[s + 1] - base) >> 5;
+    for (int k = 0; k < width; k++) {
+      const int o = base + 32 * k + lane;
+      const int c = col[o];
+      dcol[o] = (int16_t)(c >= 0 ? c - (int)r : -32768);
+    }
+  }
+}
+
 }  // namespace
+
+// Builds J->d_dcol when every stored entry lies within 32,767 of its row
+// (MTLGPU_SELL_INDEX=32 keeps 32-bit indices only).
+static mtlgpu_status sell_build_deltas(Ctx* ctx, Sell* J) {
+  if (const char* m = std::getenv("MTLGPU_SELL_INDEX"))
+    if (std::atoi(m) == 32) return MTLGPU_OK;
+  int* d_max = nullptr;
+  MTLGPU_TRY(dalloc(ctx, &d_max, 1));
+  MTLGPU_TRY_CUDA(ctx, cudaMemsetAsync(d_max, 0, sizeof(int), ctx->stream));
+  delta_max_kernel<<<grid_rows(ctx, J->n), kBlock, 0, ctx->stream>>>(J->n, J->d_slice_ptr,
+                                                                      J->d_col, d_max);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  int h_max = 0;
+  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&h_max, d_max, sizeof(int), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+  MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_max);
+  if (h_max > 32767) return MTLGPU_OK;
+  MTLGPU_TRY(dalloc(ctx, &J->d_dcol, J->n_ent));
+  dcol_fill_kernel<<<grid_rows(ctx, J->n), kBlock, 0, ctx->stream>>>(J->n, J->d_slice_ptr,
+                                                                      J->d_col, J->d_dcol);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
 
 // Padded entry count of the SELL-32 form of a CSR pattern (diag_pos as
 // sell_build), from host row pointers.
@@ -173,12 +230,13 @@ mtlgpu_status sell_build(Ctx* ctx, int n, const int32_t* d_rp, const int32_t* d_
       n, d_rp, d_ci, d_v, diag_pos, J->d_slice_ptr, J->d_col, J->d_val, J->d_val32, J->d_dinv,
       J->d_dinv32, J->round64, J->col_scaled);
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
-  return MTLGPU_OK;
+  return sell_build_deltas(ctx, J);
 }
 
 void sell_free(Ctx* ctx, Sell* J) {
   dfree(ctx, J->d_slice_ptr);
   dfree(ctx, J->d_col);
+  dfree(ctx, J->d_dcol);
   dfree(ctx, J->d_val);
   dfree(ctx, J->d_val32);
   dfree(ctx, J->d_dinv);

@@ -77,6 +77,8 @@ def _lib():
         L.mtlgpu_memcpy_h2d.argtypes = [_vp, _vp, _vp, C.c_size_t]
         L.mtlgpu_memcpy_d2h.argtypes = [_vp, _vp, _vp, C.c_size_t]
         L.mtlgpu_spmv.argtypes = [_vp, _vp, _vp, C.c_double, C.c_double]
+        L.mtlgpu_cg_direction_product.argtypes = [_vp, C.c_int, _vp, C.c_double, _vp, _vp, _vp,
+                                                  _vp]
         L.mtlgpu_axpy.argtypes = [_vp, C.c_int, C.c_double, _vp, _vp]
         L.mtlgpu_xpay.argtypes = [_vp, C.c_int, _vp, C.c_double, _vp]
         L.mtlgpu_dot.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(C.c_double)]
@@ -332,6 +334,13 @@ class Csr:
 
     def spmv_f32(self, x, y):
         check(_lib().mtlgpu_spmv_f32(self.h, x.ptr, y.ptr), "spmv_f32")
+
+    def cg_direction_product(self, prec, z, beta, p, p_out, q, pq):
+        """p_out = z + beta p (p = None: p_out = z), q = A p_out, pq[0] = p_out . q
+        (pq: a device array of at least one double)."""
+        check(_lib().mtlgpu_cg_direction_product(self.h, prec, z.ptr, beta,
+                                                 p.ptr if p is not None else None, p_out.ptr,
+                                                 q.ptr, pq.ptr), "cg_direction_product")
 
     def spmv_transposed(self, x, y):
         check(_lib().mtlgpu_spmv_transposed(self.h, x.ptr, y.ptr), "spmv_transposed")

@@ -171,3 +171,46 @@ def test_config2_mixed_jacobi_full_size(M, ctx):
     assert st == M.OK
     assert true_rel(M, A, dx.download(), b) <= 1e-10
     assert res.outer_iterations >= 2
+
+
+@pytest.mark.parametrize("prec,pc,k,A_fn", [
+    ("fp32", "ic0", 1, lambda M: M.laplacian3d(40)),
+    ("fp32", "ic0", 2, lambda M: M.fv2d(96)),
+    ("fp32", "ilu0", 3, lambda M: M.laplacian2d(80, 60)),
+    ("fp64", "ic0", 1, lambda M: M.laplacian3d(24)),
+    ("fp64", "ic0", 2, lambda M: M.fv2d(80)),
+])
+def test_fused_cg_matches_five_kernel_recording(M, ctx, monkeypatch, prec, pc, k, A_fn):
+    # CG with Jacobi-applied factors is recorded as three kernels per
+    # iteration (x/r update fused into the first L pass, p update into the
+    # product).  Against the five-kernel recording (MTLGPU_CG_FUSED=0, read
+    # when the solver's workspace is made): the same arithmetic up to the
+    # blocking of the two dot products, so the iteration counts agree to one,
+    # both solutions meet the tolerance and agree to 1e-6 (the condition
+    # number times the tolerance bounds their distance), and fewer kernels
+    # run.
+    A = A_fn(M)
+    n = A[0]
+    b = M.csr_mult(A, M.uniform(n, 1))
+    out = {}
+    for fused in (False, True):
+        if not fused:
+            monkeypatch.setenv("MTLGPU_CG_FUSED", "0")
+        else:
+            monkeypatch.delenv("MTLGPU_CG_FUSED")
+        dA = M.Csr(ctx, *A[1:])
+        P = M.Pc(dA, pc, M.FP32 if prec == "fp32" else M.FP64)
+        P.set_jacobi_sweeps(k)
+        dx, db = ctx.to_device(np.zeros(n)), ctx.to_device(b)
+        kw = dict(mode=M.SOLVE_MIXED, inner_rtol=1e-5) if prec == "fp32" else {}
+        st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=20000, **kw)
+        assert st == M.OK, (fused, st, res.iterations)
+        x = dx.download()
+        assert true_rel(M, A, x, b) <= (1e-10 if prec == "fp32" else 3e-10)
+        out[fused] = (res.iterations, res.kernel_launches, x)
+        P.close()
+        dA.close()
+    (i0, l0, x0), (i1, l1, x1) = out[False], out[True]
+    assert abs(i0 - i1) <= 1, (i0, i1)
+    assert l1 < l0, (l0, l1)
+    assert rel_err(x1, x0) <= 1e-6

@@ -103,6 +103,44 @@ def test_spmv_config_sizes(M, ctx, restate):
         dA.close()
 
 
+def banded(n, offsets, seed):
+    """CSR of an n x n matrix with entries on the given diagonals (sorted)."""
+    rng = np.random.default_rng(seed)
+    offsets = sorted(offsets)
+    rows, cols = [], []
+    for r in range(n):
+        for o in offsets:
+            if 0 <= r + o < n:
+                rows.append(r)
+                cols.append(r + o)
+    rp = np.zeros(n + 1, np.int32)
+    np.add.at(rp, np.asarray(rows) + 1, 1)
+    return n, np.cumsum(rp).astype(np.int32), np.asarray(cols, np.int32), rng.standard_normal(len(cols))
+
+
+@pytest.mark.parametrize("far", [32767, 32768])
+def test_spmv_sell_index_widths(M, ctx, restate, monkeypatch, far):
+    # The SELL-32 copy stores column indices as 16-bit offsets from the row
+    # when every entry lies within 32,767 of its row (far = 32767: the
+    # largest offset that fits), else as 32-bit indices (far = 32768).  Both
+    # sum each row in the reference's order: bit-identical products.  With
+    # MTLGPU_SELL_INDEX=32 the 16-bit copy is not built; the products agree.
+    A = banded(70000, [-far, -1, 0, 1, 5, far], 7)
+    n = A[0]
+    x = M.uniform(n, 5)
+    ref = restate.spmv(A, x)
+    got = []
+    for env in (None, "32"):
+        if env:
+            monkeypatch.setenv("MTLGPU_SELL_INDEX", env)
+        dA = M.Csr(ctx, *A[1:])
+        dx, dy = ctx.to_device(x), ctx.array(n)
+        dA.spmv(dx, dy)
+        got.append(dy.download())
+        dA.close()
+    assert np.array_equal(got[0], ref) and np.array_equal(got[1], ref)
+
+
 @pytest.mark.parametrize("A_fn", [lambda M: M.convdiff27(6, 2), lambda M: M.convdiff27(20, 2),
                                   lambda M: M.random_graph(1500, 12.0, 1e-2, 5)])
 def test_spmv_transposed(M, ctx, restate, A_fn):
@@ -311,3 +349,41 @@ def test_zero_pivot_reported(M, ctx):
     assert P.status == M.ZERO_PIVOT
     Q = M.Pc(M.Csr(ctx, rp, ci, v), "ic0")
     assert Q.status == M.ZERO_PIVOT
+
+
+@pytest.mark.parametrize("A_fn", [lambda M: M.laplacian3d(24), lambda M: M.convdiff27(12, 2)])
+def test_cg_direction_product(M, ctx, restate, A_fn):
+    # p' = z + beta p, q = A p', p'.q in one kernel (mtlgpu_cg_direction_product).
+    # FP64: p' within one rounding of z + beta p (the kernel rounds once, by
+    # fma), q bit-identical to the oracle's product of p', p'.q to 1e-14;
+    # p = None gives p' = z.  FP32: q and p'.q against FP64 arithmetic on the
+    # float-rounded values, 1e-6.
+    A = A_fn(M)
+    n, rp, ci, v = A
+    dA = M.Csr(ctx, rp, ci, v)
+    z, p, beta = M.uniform(n, 3), M.uniform(n, 4), 0.37
+    for first in (False, True):
+        dz, dp, dpo, dq, dpq = (ctx.to_device(z), ctx.to_device(p), ctx.array(n), ctx.array(n),
+                                ctx.array(1))
+        dA.cg_direction_product(M.FP64, dz, 0.0 if first else beta, None if first else dp,
+                                dpo, dq, dpq)
+        po, q, pq = dpo.download(), dq.download(), dpq.download()[0]
+        want = z if first else z + beta * p
+        assert rel_err(po, want) <= 2e-16 * 4
+        if first:
+            assert np.array_equal(po, z)
+        assert np.array_equal(q, restate.spmv(A, po))
+        assert abs(pq - np.dot(po, q)) <= 1e-14 * abs(np.dot(po, q))
+    f = lambda a: a.astype(np.float32)  # noqa: E731
+    dz, dp, dpo, dq, dpq = (ctx.to_device(f(z)), ctx.to_device(f(p)), ctx.array(n, np.float32),
+                            ctx.array(n, np.float32), ctx.array(1))
+    dA.cg_direction_product(M.FP32, dz, beta, dp, dpo, dq, dpq)
+    po, q, pq = dpo.download().astype(np.float64), dq.download().astype(np.float64), \
+        dpq.download()[0]
+    b32 = float(np.float32(beta))
+    assert rel_err(po, f(z).astype(np.float64) + b32 * f(p).astype(np.float64)) <= 1e-7
+    A32 = (n, rp, ci, f(v).astype(np.float64))
+    q64 = restate.spmv(A32, po)
+    assert rel_err(q, q64) <= 1e-6
+    assert abs(pq - np.dot(po, q)) <= 1e-6 * abs(np.dot(po, q))
+    dA.close()
