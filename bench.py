@@ -870,6 +870,23 @@ def main():
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs) / reps_
 
+    def after_ms(fn, before, reps_):
+        """Mean ms of fn launched right after before() (untimed), each fn
+        bracketed by its own CUDA events on the library's stream: fn with
+        the cache state the preceding kernels of the solve leave."""
+        evs = []
+        ctx.synchronize()
+        for _ in range(reps_):
+            before()
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            evs.append((e0, e1))
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / reps_
+
     def spmv_stats(dA_, n_, nnz_, ib_, reps_=100):
         # algorithmic bytes: 8-byte value + ib_-byte index per entry, the
         # slice offsets, x once and y once
@@ -895,7 +912,7 @@ def main():
     # update, and the U pass with r.z; the first and the last are timed here
     # (the fused L pass has no entry point of its own; its share is in the
     # launch-list profile).  Algorithmic bytes: the product reads A's entries
-    # (4-byte value + 4-byte index), the slice offsets, z and p once and
+    # (4-byte value + ib-byte index), the slice offsets, z and p once and
     # writes p and q; a Jacobi pass reads the factor's off-diagonal entries
     # (4-byte value + ib-byte index), v, D and the previous iterate once and
     # writes one vector.  The plain FP32 SpMV is timed for the record.
@@ -922,9 +939,13 @@ def main():
 
     for _ in range(5):
         direction()
-    ms_dir32, _ = timed(direction, 100)
+    # In the solve the product follows the IC(0) apply (L and U passes,
+    # ~150 MB streamed): timed that way for the roofline; back to back (L2
+    # keeps part of A between launches) and with L2 flushed, for the record.
+    ms_dir32 = after_ms(direction, lambda: P32.apply_f32(r32, z32), 50)
+    ms_dir32_b2b, _ = timed(direction, 100)
     ms_dir32_cold = cold_ms(direction, 30)
-    bytes_dir32 = nnz * 8 + 4 * (n // 32 + 1) + 4 * n * 4
+    bytes_dir32 = nnz * (4 + ib) + 4 * (n // 32 + 1) + 4 * n * 4
     traffic = read_traffic()
 
     # exact sweeps (the FP64 path's dominant kernel), for the record
@@ -973,8 +994,8 @@ def main():
         "dtype": "f32+f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": n, "nnz": nnz,
-                   "index": "int32 CSR; SELL-32 column indices: %d bytes in the FP64 "
-                            "SpMV and the Jacobi passes, 4 in the FP32 SpMV" % ib,
+                   "index": "int32 CSR; SELL-32 column indices: %d bytes in the solve's "
+                            "kernels and the FP64 SpMV, 4 in the plain FP32 SpMV" % ib,
                    "jacobi_iterations_per_triangle": JACOBI_K, "inner_rtol": INNER_RTOL,
                    "l2": "inputs larger than L2 (matrix 175 MB + factors 2 x 100 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -994,7 +1015,10 @@ def main():
                      "traffic": traffic.get(d_key), "algorithmic_bytes": d_bytes,
                      "ms": d_ms, "peak_kind": peak_kind},
         "mixed_kernels": {"cg_pspmv_f32": {"ms": ms_dir32, "GBps": bytes_dir32 / ms_dir32 / 1e6,
+                                           "how": "each launch right after an IC(0) apply, "
+                                                  "as in the solve; per-launch CUDA events",
                                            "bytes": bytes_dir32, "launches_per_iteration": 1,
+                                           "back_to_back_ms": ms_dir32_b2b,
                                            "cold_ms": ms_dir32_cold,
                                            "cold_GBps": bytes_dir32 / ms_dir32_cold / 1e6},
                           "jacobi_pass_f32": {"ms": ms_pass, "GBps": bytes_pass / ms_pass / 1e6,

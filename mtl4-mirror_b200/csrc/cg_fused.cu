@@ -38,11 +38,15 @@ using namespace dev;
 namespace {
 
 constexpr int kBlock = 256;
-// Resident blocks per SM (register budgets without spills): K_A makes two
-// gathers per entry, K_C holds 8 entries' gathers in flight.
+// Resident blocks per SM.  K_A makes two gathers per entry: 6 (40
+// registers) in FP32, 4 in FP64 (no spills).  K_C holds 8 entries' gathers
+// in flight: in FP32 6 blocks (40 registers) measured best on the 128^3
+// mixed solve (18.57 ms; 5 blocks 18.91, 4 entries per batch: 19.5-20.6);
+// in FP64 5 blocks (48 registers, no spills).
 template <typename T>
 constexpr int min_blocks_a() { return sizeof(T) == 4 ? 6 : 4; }
-constexpr int kMinBlocksC = 5;
+template <typename T>
+constexpr int min_blocks_c() { return sizeof(T) == 4 ? 6 : 5; }
 
 int rows_grid(Ctx* ctx, long long n, int per_sm) {
   const long long need = (n + kBlock - 1) / kBlock;
@@ -144,7 +148,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_a<T>())
 // num / den read from device memory (the solve's rho / rho_1), or
 // beta_value when num is null; p'.q goes to *pq.
 template <typename T, int C, bool D16, bool FIRST>
-__global__ void __launch_bounds__(kBlock, kMinBlocksC)
+__global__ void __launch_bounds__(kBlock, min_blocks_c<T>())
     cg_pspmv_kernel(int n, const int32_t* __restrict__ slice_ptr, const int32_t* __restrict__ col,
                     const int16_t* __restrict__ dcol, const T* __restrict__ val,
                     const T* __restrict__ z, const T* __restrict__ p, T* __restrict__ p_next,
@@ -212,13 +216,12 @@ struct Vals<float> {
   static float* jtmp(Pc* P) { return P->d_jtmp32; }
 };
 
-// 16-bit column offsets: in the factor passes whenever the factor has them;
-// in the product with FP64 values only (with FP32 values the 32-bit form
-// measured faster, as for the plain SpMV in spmv.cu).
-template <typename T>
-bool product_d16(const Sell& S) {
-  return S.d_dcol != nullptr && sizeof(T) == 8;
-}
+// 16-bit column offsets wherever the SELL-32 copy has them.  Measured on the
+// 128^3 mixed solve (FP32): 18.88 ms with offsets in both kernels, 18.94
+// with them in the factor pass only, 19.3-19.5 with neither; unlike the
+// plain FP32 SpMV (spmv.cu), the product with its second gather per entry
+// gains from the smaller index.
+bool product_d16(const Sell& S) { return S.d_dcol != nullptr; }
 
 struct BetaSrc {
   const int* skip;
@@ -230,9 +233,9 @@ struct BetaSrc {
 template <typename T, bool FIRST>
 void launch_pspmv(Ctx* ctx, const Sell& S, const T* val, const T* z, const T* p, T* p_next, T* q,
                   const BetaSrc& b) {
-  const int grid = rows_grid(ctx, S.n, kMinBlocksC);
+  const int grid = rows_grid(ctx, S.n, min_blocks_c<T>());
   unsigned* ctr = counter_slot(ctx, 11);
-  if (product_d16<T>(S))
+  if (product_d16(S))
     cg_pspmv_kernel<T, 8, true, FIRST><<<grid, kBlock, 0, ctx->stream>>>(
         S.n, S.d_slice_ptr, S.d_col, S.d_dcol, val, z, p, p_next, q, b.skip, b.num, b.den,
         b.value, b.pq, ctx->d_partials, ctr);
