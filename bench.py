@@ -852,12 +852,21 @@ def main():
 
     flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
 
+    def hold():
+        """Holds the library's stream with a ~20 ms spin kernel, so that a
+        loop of per-launch event pairs is queued in full before the GPU
+        reaches it: a host slower than the kernels would otherwise leave
+        idle gaps inside the event pairs."""
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(40_000_000)
+
     def cold_ms(fn, reps_):
         """Mean ms of fn with the 126 MB L2 flushed (256 MB written) before
         every launch; each launch bracketed by its own CUDA events on the
         library's stream."""
         evs = []
         ctx.synchronize()
+        hold()
         with torch.cuda.stream(stream):
             for _ in range(reps_):
                 flush.zero_()
@@ -876,6 +885,7 @@ def main():
         the cache state the preceding kernels of the solve leave."""
         evs = []
         ctx.synchronize()
+        hold()
         for _ in range(reps_):
             before()
             e0, e1 = ev(), ev()
