@@ -55,6 +55,21 @@ mtlgpu_status ctx_init(Ctx* ctx) {
     if (!std::strcmp(m, "ticket")) ctx->part_sweeps = 0;
   }
   if (const char* m = std::getenv("MTLGPU_PART_ROWS")) ctx->part_rows = std::atoi(m);
+  {
+    // the context's own pool (a failure leaves the device's default pool)
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+      unsigned long long keep = kPoolKeepBytes;
+      cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+      cudaGetLastError();
+      ctx->pool = nullptr;
+    }
+  }
   MTLGPU_TRY(dalloc(ctx, &ctx->d_partials, (size_t)kMaxPartials * kPartialWidth));
   MTLGPU_TRY(dalloc(ctx, &ctx->d_counters, kNumCounters));
   MTLGPU_TRY(dalloc(ctx, &ctx->d_scalars, 64));
@@ -211,6 +226,9 @@ mtlgpu_status mtlgpu_ctx_destroy(mtlgpu_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->h_scalars) cudaFreeHost(c->h_scalars);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  // memory still held by handles of this context is released with the
+  // pool once those handles free it
+  if (c->pool) cudaMemPoolDestroy(c->pool);
   delete c;
   return MTLGPU_OK;
 }

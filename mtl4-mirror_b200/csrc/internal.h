@@ -19,6 +19,8 @@ constexpr int kPartialWidth = 4;
 // Number of independent "last block" counters (one per reduction site that
 // may be in flight in one stream-ordered sequence).
 constexpr int kNumCounters = 64;
+// Freed device memory a context's pool keeps mapped for reuse.
+constexpr unsigned long long kPoolKeepBytes = 4ull << 30;
 
 struct Ctx {
   int device = 0;
@@ -33,6 +35,11 @@ struct Ctx {
   double* d_scalars = nullptr;    // 64 scalar result slots
   double* h_scalars = nullptr;    // pinned mirror (64)
   int* d_error = nullptr;         // device error word: 0 ok, else mtlgpu_status
+  // Stream-ordered pool for every device allocation of this context.  Freed
+  // memory stays mapped up to kPoolKeepBytes, so per-call scratch (the
+  // staging vectors of mtlgpu_solve_host, temporary arrays) is not unmapped
+  // and mapped again at every synchronisation as with the default pool.
+  cudaMemPool_t pool = nullptr;
   long long launches = 0;         // kernels launched on this context (host-side count)
   // Resident CTAs per SM for the triangular sweeps (fewer pollers contend
   // less for L2; 2 measured best on B200).  Benchmark override:
@@ -201,7 +208,10 @@ template <typename T>
 mtlgpu_status dalloc(Ctx* ctx, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), count * sizeof(T), ctx->stream);
+  cudaError_t e =
+      ctx->pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), count * sizeof(T),
+                                          ctx->pool, ctx->stream)
+                : cudaMallocAsync(reinterpret_cast<void**>(p), count * sizeof(T), ctx->stream);
   if (e != cudaSuccess) {
     ctx->last_error = std::string("device allocation failed: ") + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? MTLGPU_OUT_OF_MEMORY : MTLGPU_CUDA_ERROR;
