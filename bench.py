@@ -628,8 +628,9 @@ def profile_case(case, grid, launches):
     'spmv32' (FP32), 'jacobi32' (FP32 IC(0) apply with JACOBI_K Jacobi
     iterations per triangle), 'sweep64' / 'sweep32' (exact IC(0) lower sweep),
     'mixed' (complete mixed solves of the headline configuration, for the
-    launch list), 'batched' (the 512-system batched Jacobi PCG, FP64),
-    'assemble' (device assembly of the N^3 Laplacian from shuffled triplets)."""
+    launch list), 'mixed27' (the mixed BiCGSTAB + ILU(0) solve of the N^3
+    27-point convection-diffusion system, seed 2), 'batched' (the 512-system
+    batched Jacobi PCG, FP64), 'assemble' (device assembly of the N^3 Laplacian from shuffled triplets)."""
     import mtlgpu as M
     A = M.laplacian3d(grid)
     n = A[0]
@@ -654,6 +655,20 @@ def profile_case(case, grid, launches):
         for _ in range(launches):
             dx.upload(np.zeros(n))
             st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=4000,
+                                 mode=M.SOLVE_MIXED, inner_rtol=INNER_RTOL)
+            assert st == M.OK, st
+    elif case == "mixed27":
+        A = M.convdiff27(grid, 2)
+        n = A[0]
+        dA.close()
+        dA = M.Csr(ctx, *A[1:])
+        P = M.Pc(dA, "ilu0", M.FP32)
+        P.set_jacobi_sweeps(JACOBI_K)
+        b = M.csr_mult(A, M.uniform(n, 1))
+        dx, db = ctx.array(n), ctx.to_device(b)
+        for _ in range(launches):
+            dx.upload(np.zeros(n))
+            st, res, _ = M.solve("bicgstab", dA, P, dx, db, rtol=1e-10, max_iter=4000,
                                  mode=M.SOLVE_MIXED, inner_rtol=INNER_RTOL)
             assert st == M.OK, st
     elif case == "assemble":
@@ -738,7 +753,7 @@ def main():
                     help="skip the config-3, batched and differentiable-solve measurements")
     ap.add_argument("--profile-case",
                     choices=["spmv", "spmv32", "jacobi32", "sweep64", "sweep32", "mixed",
-                             "batched", "assemble"])
+                             "mixed27", "batched", "assemble"])
     ap.add_argument("--sweep-scan", action="store_true",
                     help="per-level cost of the exact sweep on 64^3 .. 192^3 grids")
     ap.add_argument("--grid", type=int, default=64)

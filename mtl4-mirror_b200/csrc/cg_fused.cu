@@ -223,6 +223,60 @@ struct Vals<float> {
 // gains from the smaller index.
 bool product_d16(const Sell& S) { return S.d_dcol != nullptr; }
 
+// BiCGSTAB's t = A shat with omega's two dots, t.s and t.t (bicgstab.hpp:
+// 69-70), in one pass: the product is spmv_sell's; the dots replace the
+// separate omega kernel of the unfused recording (their blocking differs
+// from that kernel's, so omega may differ in its last bits: used only with
+// Jacobi-applied factors, whose solves are not held to the reference's
+// iteration counts).
+template <typename T, int C, bool D16>
+__global__ void __launch_bounds__(kBlock, min_blocks_c<T>())
+    bicg_tprod_kernel(int n, const int32_t* __restrict__ slice_ptr,
+                      const int32_t* __restrict__ col, const int16_t* __restrict__ dcol,
+                      const T* __restrict__ val, const T* __restrict__ shat,
+                      const T* __restrict__ s, T* __restrict__ t, SolverState* st, void* partials,
+                      unsigned* counter) {
+  if (st->done || st->skip2) return;
+  typedef typename AccOf<T, 2>::type R;
+  R acc = R::zero();
+  for (long long rl = gtid(); rl < n; rl += gstride()) {
+    const int row = (int)rl;
+    const int lane = row & 31;
+    const int sl = row >> 5;
+    const int base = __ldg(slice_ptr + sl);
+    const int width = (__ldg(slice_ptr + sl + 1) - base) >> 5;
+    T sum = T(0);
+    for (int k0 = 0; k0 < width; k0 += C) {
+      int c[C];
+      T a[C], g[C];
+#pragma unroll
+      for (int u = 0; u < C; u++) {
+        const bool in = k0 + u < width;
+        const int o = base + 32 * (k0 + u) + lane;
+        c[u] = sell_col<D16>(col, dcol, o, row, in);
+        a[u] = in ? __ldlu(val + o) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < C; u++) g[u] = c[u] >= 0 ? __ldg(shat + c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < C; u++)
+        if (c[u] >= 0) sum = add_rn(sum, mul_rn(a[u], g[u]));
+    }
+    t[row] = sum;
+    acc.add_prod(0, sum, __ldg(s + row));
+    acc.add_prod(1, sum, sum);
+  }
+  R bs = block_reduce(acc);
+  R* parts = reinterpret_cast<R*>(partials);
+  if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
+    R tot = reduce_partials(parts, gridDim.x);
+    if (threadIdx.x == 0) {
+      st->ts = tot.value(0);
+      st->tt = tot.value(1);
+    }
+  }
+}
+
 struct BetaSrc {
   const int* skip;
   const double *num, *den;  // beta = *num / *den, or value when num is null
@@ -328,6 +382,29 @@ mtlgpu_status cg_fused_iteration(Csr* A, Pc* P, SolverState* st, T* x, const T* 
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
 }
+
+template <typename T>
+mtlgpu_status bicg_t_product(Csr* A, SolverState* st, const T* shat, const T* s, T* t) {
+  Ctx* ctx = A->ctx;
+  const Sell& S = A->sell;
+  const T* val = Vals<T>::val(S);
+  const int grid = rows_grid(ctx, S.n, min_blocks_c<T>());
+  unsigned* ctr = counter_slot(ctx, 12);
+  if (product_d16(S))
+    bicg_tprod_kernel<T, 8, true><<<grid, kBlock, 0, ctx->stream>>>(
+        S.n, S.d_slice_ptr, S.d_col, S.d_dcol, val, shat, s, t, st, ctx->d_partials, ctr);
+  else
+    bicg_tprod_kernel<T, 8, false><<<grid, kBlock, 0, ctx->stream>>>(
+        S.n, S.d_slice_ptr, S.d_col, S.d_dcol, val, shat, s, t, st, ctx->d_partials, ctr);
+  ctx->launches++;
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  return MTLGPU_OK;
+}
+
+template mtlgpu_status bicg_t_product<double>(Csr*, SolverState*, const double*, const double*,
+                                              double*);
+template mtlgpu_status bicg_t_product<float>(Csr*, SolverState*, const float*, const float*,
+                                             float*);
 
 // p' = z + beta p (p' = z when p is null), q = A p', *d_pq = p'.q: the
 // product kernel of the fused CG on its own (mtlgpu_cg_direction_product).

@@ -308,13 +308,19 @@ __global__ void __launch_bounds__(kBlock, 4)
 
 // x += omega shat + alpha phat, r = s - omega t, ||r|| and the loop test
 // (bicgstab.hpp:70-75, 43); on a half-step exit only x += alpha phat.
+// The next iteration's start is folded in: rho_1 = rtilde . r over the new
+// r (component 1 of the same reduction; component 0 is ||r||^2, summed as
+// alone), the breakdown tests and ++iter of bicg_rho_kernel, and the reset
+// of skip2.  The grid and the element order are bicg_rho_kernel's, so rho_1
+// has the same bits as that kernel's.
 template <typename T>
 __global__ void __launch_bounds__(kBlock, 4)
     bicg_x_kernel(int n, T* __restrict__ x, const T* __restrict__ phat, const T* __restrict__ shat,
-                  const T* __restrict__ s, const T* __restrict__ t, T* __restrict__ r, T* fill_a,
-                  T* fill_b, SolverState* st, void* partials, unsigned* counter) {
+                  const T* __restrict__ s, const T* __restrict__ t, T* __restrict__ r,
+                  const T* __restrict__ rt, T* fill_a, T* fill_b, SolverState* st, void* partials,
+                  unsigned* counter) {
   if (st->done) return;
-  typedef typename AccOf<T, 1>::type R;
+  typedef typename AccOf<T, 2>::type R;
   const T alpha = (T)st->alpha_1;
   constexpr int V = VN<T>::value;
   if (st->half_exit) {
@@ -346,10 +352,14 @@ __global__ void __launch_bounds__(kBlock, 4)
     ld16(s + i0, sv);
     ld16(t + i0, tv);
 #pragma unroll
+    T rtv[V];
+    ld16(rt + i0, rtv);
+#pragma unroll
     for (int u = 0; u < V; u++) {
       xv[u] += omega * sh[u] + alpha * ph[u];
       sv[u] = sv[u] - omega * tv[u];  // r
       acc.add_prod(0, sv[u], sv[u]);
+      acc.add_prod(1, rtv[u], sv[u]);
       fv[u] = sent;
     }
     st16(x + i0, xv);
@@ -362,6 +372,7 @@ __global__ void __launch_bounds__(kBlock, 4)
     const T ri = s[i] - omega * t[i];
     r[i] = ri;
     acc.add_prod(0, ri, ri);
+    acc.add_prod(1, rt[i], ri);
     if (fill_a) fill_a[i] = sent;
     if (fill_b) fill_b[i] = sent;
   }
@@ -375,6 +386,18 @@ __global__ void __launch_bounds__(kBlock, 4)
       const double rr = tot.value(0);
       st->rr = rr;
       if (iter_finished(st, sqrt(rr))) st->done = 1;
+      // the next iteration's start (bicg_rho_kernel, bicg_reset_skip_kernel)
+      st->skip2 = st->done ? 1 : 0;
+      if (!st->done) {
+        st->iter++;
+        const double rho1 = tot.value(1);
+        st->rho = rho1;
+        if (rho1 == 0.0 || (st->iter > 1 && st->omega == 0.0)) {
+          st->status = MTLGPU_BREAKDOWN;
+          st->done = 1;
+          st->skip2 = 1;
+        }
+      }
     }
   }
 }
@@ -557,9 +580,8 @@ mtlgpu_status record_bicgstab_iteration(Workspace<T>* W) {
   const int grid = vec_grid(ctx, n);
   const bool sw = uses_sweeps(W->P);
   T* tmp = pc_tmp<T>(W->P);
-  bicg_reset_skip_kernel<<<1, 32, 0, ctx->stream>>>(W->st);
-  bicg_rho_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->rt, W->r, W->st, ctx->d_partials,
-                                                       counter_slot(ctx, 3));
+  // rho_1 and the skip reset of this iteration were made by the previous
+  // iteration's x update (the first iteration's by bicgstab_prologue)
   bicg_p_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->p, W->v, W->st);
   // phat = solve(M, p)  (sweep outputs prefilled by the previous x-update)
   MTLGPU_TRY(apply_pc<T>(W, W->p, W->phat, &W->st->done, sw));
@@ -574,15 +596,20 @@ mtlgpu_status record_bicgstab_iteration(Workspace<T>* W) {
                                                      ctx->d_partials, counter_slot(ctx, 4));
   // shat = solve(M, s); t = A shat; omega
   MTLGPU_TRY(apply_pc<T>(W, W->s, W->shat, &W->st->skip2, sw));
-  SpmvArgs a2;
-  a2.epi = EPI_AXPBY;
-  a2.skip = &W->st->skip2;
-  MTLGPU_TRY(spmv_launch<T>(A, W->shat, W->t, a2));
-  bicg_omega_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->t, W->s, W->st, ctx->d_partials,
-                                                         counter_slot(ctx, 5));
+  if (W->fused) {
+    MTLGPU_TRY(bicg_t_product<T>(A, W->st, W->shat, W->s, W->t));  // t and omega's dots
+  } else {
+    SpmvArgs a2;
+    a2.epi = EPI_AXPBY;
+    a2.skip = &W->st->skip2;
+    MTLGPU_TRY(spmv_launch<T>(A, W->shat, W->t, a2));
+    bicg_omega_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->t, W->s, W->st,
+                                                           ctx->d_partials, counter_slot(ctx, 5));
+  }
   bicg_x_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->x, W->phat, W->shat, W->s, W->t, W->r,
-                                                     sw ? tmp : nullptr, sw ? W->phat : nullptr,
-                                                     W->st, ctx->d_partials, counter_slot(ctx, 6));
+                                                     W->rt, sw ? tmp : nullptr,
+                                                     sw ? W->phat : nullptr, W->st,
+                                                     ctx->d_partials, counter_slot(ctx, 6));
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
 }
@@ -630,7 +657,7 @@ mtlgpu_status alloc_workspace(Workspace<T>* W) {
   MTLGPU_TRY(dalloc(ctx, &W->p, n));
   MTLGPU_TRY(dalloc(ctx, &W->q, n));
   if (!is_identity(W->P) || W->method == MTLGPU_BICGSTAB) MTLGPU_TRY(dalloc(ctx, &W->z, n));
-  if (W->fused) {
+  if (W->fused && W->method == MTLGPU_CG) {
     MTLGPU_TRY(dalloc(ctx, &W->r2, n));
     MTLGPU_TRY(dalloc(ctx, &W->p2, n));
   }
@@ -688,7 +715,7 @@ mtlgpu_status get_workspace(Csr* A, Pc* P, int method, Workspace<T>** out) {
   W->P = P;
   W->method = method;
   W->n = A->n_rows;
-  W->fused = method == MTLGPU_CG && cg_fused_eligible(A, P, prec);
+  W->fused = (method == MTLGPU_CG || method == MTLGPU_BICGSTAB) && cg_fused_eligible(A, P, prec);
   mtlgpu_status s = alloc_workspace<T>(W);
   if (s != MTLGPU_OK) {
     release_workspace<T>(W);
@@ -805,7 +832,15 @@ mtlgpu_status device_solve(Workspace<T>* W, const mtlgpu_iter_params* prm, doubl
     ctx->launches++;
   }
   // the fused recording starts inside the first iteration (z, rho, p, q)
-  if (W->fused) MTLGPU_TRY(cg_fused_prologue<T>(A, W->P, W->st, W->r, W->z, W->p, W->q));
+  if (W->fused && W->method == MTLGPU_CG)
+    MTLGPU_TRY(cg_fused_prologue<T>(A, W->P, W->st, W->r, W->z, W->p, W->q));
+  // BiCGSTAB's first rho_1 (later ones come with the x update)
+  if (W->method == MTLGPU_BICGSTAB) {
+    bicg_reset_skip_kernel<<<1, 32, 0, ctx->stream>>>(W->st);
+    bicg_rho_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->rt, W->r, W->st, ctx->d_partials,
+                                                         counter_slot(ctx, 3));
+    ctx->launches += 2;
+  }
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   int interrupted = 0;
   MTLGPU_TRY(run_iterations<T>(W, prm->h_interrupt, &interrupted));

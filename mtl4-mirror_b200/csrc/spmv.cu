@@ -525,10 +525,12 @@ mtlgpu_status spmv_launch(Csr* A, const T* x, T* y, const SpmvArgs& args) {
     ep.part_off = 0;
     ep.part_total = grid;
     ep.final_launch = true;
-    // 16-bit indices for FP64 values only: measured on the 128^3 Laplacian
-    // they take the FP64 product from 31.8 to 28.7 us (cold L2: 43.5 to
-    // 38.3), while the FP32 product, back to back, slows from 22.9 to 24.6.
-    if (A->sell.d_dcol && sizeof(T) == 8)
+    // 16-bit indices for FP64 values, and for FP32 values with rows wider
+    // than 8 entries.  Measured: the 128^3 7-point FP64 product from 31.8 to
+    // 28.7 us (cold L2: 43.5 to 38.3), while its FP32 product, back to back,
+    // slows from 22.9 to 24.6; the 96^3 27-point FP32 product goes from 33.2
+    // to 32.8 us (config-3 mixed solve 14.28 to 14.01 ms).
+    if (A->sell.d_dcol && (sizeof(T) == 8 || A->sell.max_width > 8))
       spmv_sell<T, 8, true><<<grid, kBlock, 0, ctx->stream>>>(
           A->n_rows, A->sell.d_slice_ptr, A->sell.d_col, A->sell.d_dcol, sv, x, y, ep);
     else

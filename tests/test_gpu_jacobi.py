@@ -173,19 +173,22 @@ def test_config2_mixed_jacobi_full_size(M, ctx):
     assert res.outer_iterations >= 2
 
 
-@pytest.mark.parametrize("prec,pc,k,A_fn", [
-    ("fp32", "ic0", 1, lambda M: M.laplacian3d(40)),
-    ("fp32", "ic0", 2, lambda M: M.fv2d(96)),
-    ("fp32", "ilu0", 3, lambda M: M.laplacian2d(80, 60)),
-    ("fp64", "ic0", 1, lambda M: M.laplacian3d(24)),
-    ("fp64", "ic0", 2, lambda M: M.fv2d(80)),
+@pytest.mark.parametrize("method,prec,pc,k,A_fn", [
+    ("cg", "fp32", "ic0", 1, lambda M: M.laplacian3d(40)),
+    ("cg", "fp32", "ic0", 2, lambda M: M.fv2d(96)),
+    ("cg", "fp32", "ilu0", 3, lambda M: M.laplacian2d(80, 60)),
+    ("cg", "fp64", "ic0", 1, lambda M: M.laplacian3d(24)),
+    ("cg", "fp64", "ic0", 2, lambda M: M.fv2d(80)),
+    ("bicgstab", "fp32", "ilu0", 1, lambda M: M.convdiff27(20, 2)),
+    ("bicgstab", "fp64", "ilu0", 2, lambda M: M.convdiff27(16, 2)),
 ])
-def test_fused_cg_matches_five_kernel_recording(M, ctx, monkeypatch, prec, pc, k, A_fn):
+def test_fused_cg_matches_five_kernel_recording(M, ctx, monkeypatch, method, prec, pc, k, A_fn):
     # CG with Jacobi-applied factors is recorded as three kernels per
     # iteration (x/r update fused into the first L pass, p update into the
-    # product).  Against the five-kernel recording (MTLGPU_CG_FUSED=0, read
-    # when the solver's workspace is made): the same arithmetic up to the
-    # blocking of the two dot products, so the iteration counts agree to one,
+    # product); BiCGSTAB's t = A shat carries omega's two dots.  Against the
+    # unfused recording (MTLGPU_CG_FUSED=0, read when the solver's workspace
+    # is made): the same arithmetic up to the blocking of the dot products
+    # that moved, so the iteration counts agree to one,
     # both solutions meet the tolerance and agree to 1e-6 (the condition
     # number times the tolerance bounds their distance), and fewer kernels
     # run.
@@ -203,7 +206,7 @@ def test_fused_cg_matches_five_kernel_recording(M, ctx, monkeypatch, prec, pc, k
         P.set_jacobi_sweeps(k)
         dx, db = ctx.to_device(np.zeros(n)), ctx.to_device(b)
         kw = dict(mode=M.SOLVE_MIXED, inner_rtol=1e-5) if prec == "fp32" else {}
-        st, res, _ = M.solve("cg", dA, P, dx, db, rtol=1e-10, max_iter=20000, **kw)
+        st, res, _ = M.solve(method, dA, P, dx, db, rtol=1e-10, max_iter=20000, **kw)
         assert st == M.OK, (fused, st, res.iterations)
         x = dx.download()
         assert true_rel(M, A, x, b) <= (1e-10 if prec == "fp32" else 3e-10)
