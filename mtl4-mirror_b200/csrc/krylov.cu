@@ -9,7 +9,11 @@
 // returns at once when the state says the solve has finished.  The host
 // launches a graph of kGraphIters iterations at a time and only looks at the
 // state between graph launches (that is also where the interrupt flag is
-// polled, as itl::interruptible_iteration does between iterations).
+// polled, as itl::interruptible_iteration does between iterations).  Without
+// an interrupt flag the iterations run in a device-side loop instead: one
+// launch of a graph whose conditional WHILE node repeats the kGraphIters
+// iterations until the state says done (or an error is raised, or a trip
+// bound derived from max_iter is reached), with no host round trip between.
 //
 // Per CG iteration (preconditioned):
 //   sweeps   y0 = L^-1 r, z = U^-1 y0          (sweep.cu)
@@ -34,7 +38,9 @@ namespace mtlgpu {
 
 using namespace dev;
 
-constexpr int kGraphIters = 8;
+// Iterations per graph (per body of the device-side loop): 16 measured
+// 0.22 ms faster than 8 on the 128^3 mixed solve, 32 no faster than 16.
+constexpr int kGraphIters = 16;
 // The fused CG recording alternates two r and two p buffers by iteration
 // parity; an even count per graph keeps the parity across graph launches.
 static_assert(kGraphIters % 2 == 0, "graphs hold an even number of iterations");
@@ -491,6 +497,8 @@ struct Workspace {
   int hist_cap = 0;
   cudaGraphExec_t exec = nullptr;
   size_t graph_nodes = 0;      // kernel nodes per graph launch
+  cudaGraphExec_t exec_loop = nullptr;  // the same iterations in a device-side loop
+  bool loop_failed = false;             // the loop graph could not be made: host loop
   ~Workspace() {}
 };
 
@@ -647,6 +655,61 @@ mtlgpu_status build_graph(Workspace<T>* W) {
   return MTLGPU_OK;
 }
 
+// Condition of the device-side loop: run the body again unless the solve
+// is over, an error was raised or the trip bound is reached.
+__global__ void loop_cond_kernel(cudaGraphConditionalHandle h, SolverState* st, const int* err) {
+  const int trips = ++st->trips;
+  const bool more = !st->done && !*err && trips < st->max_trips;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// One graph: a WHILE node whose body is kGraphIters iterations and the
+// condition kernel.
+template <typename T>
+mtlgpu_status build_loop_graph(Workspace<T>* W) {
+  Ctx* ctx = W->A->ctx;
+  cudaGraph_t g = nullptr;
+  MTLGPU_TRY_CUDA(ctx, cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    MTLGPU_TRY_CUDA(ctx, e);
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  const long long launches_before = ctx->launches;
+  e = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    MTLGPU_TRY_CUDA(ctx, e);
+  }
+  mtlgpu_status s = MTLGPU_OK;
+  for (int k = 0; k < kGraphIters && s == MTLGPU_OK; k++)
+    s = W->method == MTLGPU_CG ? record_cg_iteration<T>(W, k) : record_bicgstab_iteration<T>(W);
+  if (s == MTLGPU_OK) loop_cond_kernel<<<1, 1, 0, ctx->stream>>>(h, W->st, ctx->d_error);
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(ctx->stream, &captured);
+  ctx->launches = launches_before;
+  if (s != MTLGPU_OK || e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    if (s != MTLGPU_OK) return s;
+    MTLGPU_TRY_CUDA(ctx, e);
+  }
+  e = cudaGraphInstantiate(&W->exec_loop, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) W->exec_loop = nullptr;
+  MTLGPU_TRY_CUDA(ctx, e);
+  return MTLGPU_OK;
+}
+
 template <typename T>
 mtlgpu_status alloc_workspace(Workspace<T>* W) {
   Ctx* ctx = W->A->ctx;
@@ -681,6 +744,7 @@ void release_workspace(Workspace<T>* W) {
   if (!W) return;
   Ctx* ctx = W->A->ctx;
   if (W->exec) cudaGraphExecDestroy(W->exec);
+  if (W->exec_loop) cudaGraphExecDestroy(W->exec_loop);
   T** bufs[] = {&W->x, &W->b, &W->r, &W->z, &W->p, &W->q, &W->rt, &W->phat, &W->s, &W->shat,
                 &W->t, &W->v, &W->r2, &W->p2};
   for (T** b : bufs) dfree(ctx, *b);
@@ -745,6 +809,29 @@ mtlgpu_status run_iterations(Workspace<T>* W, const volatile int* h_interrupt, i
   Ctx* ctx = W->A->ctx;
   MTLGPU_TRY(build_graph<T>(W));
   *interrupted = 0;
+  if (!h_interrupt && !W->loop_failed && !W->exec_loop &&
+      build_loop_graph<T>(W) != MTLGPU_OK) {
+    // keep the host loop for this workspace
+    W->loop_failed = true;
+    cudaGetLastError();
+    ctx->last_error.clear();
+  }
+  if (!h_interrupt && W->exec_loop) {
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->h_st, W->st, sizeof(SolverState),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (W->h_st->done) return take_device_error(ctx);
+    MTLGPU_TRY_CUDA(ctx, cudaGraphLaunch(W->exec_loop, ctx->stream));
+    int err = 0;
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->h_st, W->st, sizeof(SolverState),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->launches += (long long)W->h_st->trips * (long long)(W->graph_nodes + 1);
+    if (err || W->h_st->done) return take_device_error(ctx);
+    // the trip bound ended the loop first: the host loop below carries on
+  }
   while (true) {
     MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(W->h_st, W->st, sizeof(SolverState),
                                          cudaMemcpyDeviceToHost, ctx->stream));
@@ -772,6 +859,9 @@ void init_state(SolverState* h, const mtlgpu_iter_params* prm, double norm_r0, i
                 double* history, int hist_cap) {
   std::memset(h, 0, sizeof(SolverState));
   h->max_iter = max_iter;
+  // every body run of the device-side loop makes kGraphIters iterations
+  // unless the solve has ended, so max_iter bounds the runs
+  h->max_trips = max_iter / kGraphIters + 4;
   h->tol = prm->rtol * norm_r0;
   h->atol = prm->atol;
   h->norm_r0 = norm_r0;

@@ -16,7 +16,8 @@ struct SolverState {
   int max_iter;
   int hist_len;
   int hist_cap;
-  int pad;
+  int trips;      // device-side graph loop: body runs so far
+  int max_trips;  //   and the bound past which the loop stops
   double tol;     // rtol * norm_r0
   double atol;
   double norm_r0;
