@@ -86,7 +86,11 @@ __device__ __forceinline__ int sell_col(const int32_t* __restrict__ col,
 
 // K_A.  The Jacobi pass is jacobi_pass_kernel's (same chunking, same
 // accumulation), with v = r' and its gathers formed from r and q.
-template <typename T, bool SCALE, int C, bool D16>
+// BICG: the same kernel makes BiCGSTAB's s = r - alpha v (q = v, r_next = s,
+// no x update; alpha = rho / gamma) with ||s||^2 and the half-step test of
+// bicgstab.hpp:58-67 (bicg_s_kernel's), fused into the first L pass of
+// shat = solve(M, s).
+template <typename T, bool SCALE, int C, bool D16, bool BICG>
 __global__ void __launch_bounds__(kBlock, min_blocks_a<T>())
     cg_lupd_kernel(int n, const int32_t* __restrict__ slice_ptr, const int32_t* __restrict__ col,
                    const int16_t* __restrict__ dcol, const T* __restrict__ val,
@@ -95,7 +99,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_a<T>())
                    T* __restrict__ out, SolverState* st, void* partials, unsigned* counter) {
   if (st->done) return;
   typedef typename AccOf<T, 1>::type R;
-  const T alpha = (T)(st->rho / st->alpha_1);
+  const double gamma = st->gamma;
+  const T alpha = (T)(BICG ? st->rho / gamma : st->rho / st->alpha_1);
   R acc_rr = R::zero();
   for (long long rl = gtid(); rl < n; rl += gstride()) {
     const int row = (int)rl;
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_a<T>())
     const T rv = next_r(__ldg(r + row), __ldg(q + row), alpha);
     const T dr = SCALE ? __ldg(dinv + row) : T(1);
     r_next[row] = rv;
-    x[row] = fma_t(alpha, __ldg(p + row), x[row]);
+    if (!BICG) x[row] = fma_t(alpha, __ldg(p + row), x[row]);
     acc_rr.add_prod(0, rv, rv);
     T acc = T(0);
     for (int k0 = 0; k0 < width; k0 += C) {
@@ -134,11 +139,26 @@ __global__ void __launch_bounds__(kBlock, min_blocks_a<T>())
   if (publish_partial(bs, parts, blockIdx.x, counter, gridDim.x)) {
     R tot = reduce_partials(parts, gridDim.x);
     if (threadIdx.x == 0) {
-      const double rr = tot.value(0);
-      st->iter++;
-      st->rho_1 = st->rho;
-      st->rr = rr;
-      if (iter_finished(st, sqrt(fabs(rr)))) st->done = 1;
+      if (BICG) {
+        if (gamma == 0.0) {
+          st->status = MTLGPU_BREAKDOWN;
+          st->done = 1;
+          st->skip2 = 1;
+        } else {
+          st->alpha_1 = st->rho / gamma;  // alpha
+          st->ss = tot.value(0);
+          if (iter_finished(st, sqrt(st->ss))) {
+            st->half_exit = 1;
+            st->skip2 = 1;
+          }
+        }
+      } else {
+        const double rr = tot.value(0);
+        st->iter++;
+        st->rho_1 = st->rho;
+        st->rr = rr;
+        if (iter_finished(st, sqrt(fabs(rr)))) st->done = 1;
+      }
     }
   }
 }
@@ -304,29 +324,58 @@ BetaSrc state_beta(SolverState* st) {
   return BetaSrc{&st->done, &st->rho, &st->rho_1, 0.0, &st->alpha_1};
 }
 
-template <typename T, bool SCALE, int C>
+template <typename T, bool SCALE, int C, bool BICG>
 void launch_lupd_c(Ctx* ctx, const Sell& L, const T* val, const T* dinv, T* x, const T* p,
                    const T* r, const T* q, T* r_next, T* out, SolverState* st) {
   const int grid = rows_grid(ctx, L.n, min_blocks_a<T>());
   unsigned* ctr = counter_slot(ctx, 10);
   if (L.d_dcol)
-    cg_lupd_kernel<T, SCALE, C, true><<<grid, kBlock, 0, ctx->stream>>>(
+    cg_lupd_kernel<T, SCALE, C, true, BICG><<<grid, kBlock, 0, ctx->stream>>>(
         L.n, L.d_slice_ptr, L.d_col, L.d_dcol, val, dinv, x, p, r, q, r_next, out, st,
         ctx->d_partials, ctr);
   else
-    cg_lupd_kernel<T, SCALE, C, false><<<grid, kBlock, 0, ctx->stream>>>(
+    cg_lupd_kernel<T, SCALE, C, false, BICG><<<grid, kBlock, 0, ctx->stream>>>(
         L.n, L.d_slice_ptr, L.d_col, L.d_dcol, val, dinv, x, p, r, q, r_next, out, st,
         ctx->d_partials, ctr);
   ctx->launches++;
 }
 
-template <typename T, bool SCALE>
+template <typename T, bool SCALE, bool BICG>
 void launch_lupd(Ctx* ctx, const Sell& L, const T* val, const T* dinv, T* x, const T* p,
                  const T* r, const T* q, T* r_next, T* out, SolverState* st) {
   if (L.max_width <= 4)
-    launch_lupd_c<T, SCALE, 4>(ctx, L, val, dinv, x, p, r, q, r_next, out, st);
+    launch_lupd_c<T, SCALE, 4, BICG>(ctx, L, val, dinv, x, p, r, q, r_next, out, st);
   else
-    launch_lupd_c<T, SCALE, 8>(ctx, L, val, dinv, x, p, r, q, r_next, out, st);
+    launch_lupd_c<T, SCALE, 8, BICG>(ctx, L, val, dinv, x, p, r, q, r_next, out, st);
+}
+
+// The first L pass of solve(M, v') where v' = v0 - alpha w is formed in the
+// pass (CG: r' and the x update; BiCGSTAB: s), then the remaining passes
+// and the U triangle; the U triangle's last pass reduces dot_with . z into
+// *dot_out when dot_with is given.  skip2: the passes after the first skip
+// on it (BiCGSTAB's half-step exit), else on done.
+template <typename T, bool BICG>
+mtlgpu_status fused_apply(Ctx* ctx, Pc* P, SolverState* st, T* x, const T* p, const T* v0,
+                          const T* w, T* v_next, T* z, const int* skip_rest, const T* dot_with,
+                          double* dot_out) {
+  const int k = P->jacobi_iters;
+  const Sell& L = P->jac_lower;
+  T* tmp = Vals<T>::tmp(P);
+  T* scratch = Vals<T>::jtmp(P);
+  // pass 0 of the L triangle writes where jacobi_solve would: tmp when it is
+  // the only pass (k odd), else scratch
+  T* out0 = (k % 2 == 1) ? tmp : scratch;
+  const T* val = Vals<T>::val(L);
+  const T* dinv = Vals<T>::dinv(L);
+  if (k == 1 && !L.unit_diag)
+    launch_lupd<T, true, BICG>(ctx, L, val, dinv, x, p, v0, w, v_next, out0, st);
+  else
+    launch_lupd<T, false, BICG>(ctx, L, val, dinv, x, p, v0, w, v_next, out0, st);
+  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
+  if (k > 1) MTLGPU_TRY(jacobi_solve_from<T>(ctx, L, k, 1, v_next, tmp, scratch, skip_rest));
+  MTLGPU_TRY(jacobi_solve<T>(ctx, P->jac_upper, k, tmp, z, scratch, skip_rest, dot_with,
+                             dot_out));
+  return MTLGPU_OK;
 }
 
 }  // namespace
@@ -362,26 +411,26 @@ template <typename T>
 mtlgpu_status cg_fused_iteration(Csr* A, Pc* P, SolverState* st, T* x, const T* r, T* r_next,
                                  const T* p, T* p_next, T* z, T* q) {
   Ctx* ctx = A->ctx;
-  const int k = P->jacobi_iters;
-  const Sell& L = P->jac_lower;
-  T* tmp = Vals<T>::tmp(P);
-  T* scratch = Vals<T>::jtmp(P);
-  // pass 0 of the L triangle writes where jacobi_solve would: tmp when it is
-  // the only pass (k odd), else scratch
-  T* out0 = (k % 2 == 1) ? tmp : scratch;
-  const T* val = Vals<T>::val(L);
-  const T* dinv = Vals<T>::dinv(L);
-  if (k == 1 && !L.unit_diag)
-    launch_lupd<T, true>(ctx, L, val, dinv, x, p, r, q, r_next, out0, st);
-  else
-    launch_lupd<T, false>(ctx, L, val, dinv, x, p, r, q, r_next, out0, st);
-  MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
-  if (k > 1) MTLGPU_TRY(jacobi_solve_from<T>(ctx, L, k, 1, r_next, tmp, scratch, &st->done));
-  MTLGPU_TRY(jacobi_solve<T>(ctx, P->jac_upper, k, tmp, z, scratch, &st->done, r_next, &st->rho));
+  MTLGPU_TRY((fused_apply<T, false>(ctx, P, st, x, p, r, q, r_next, z, &st->done, r_next,
+                                    &st->rho)));
   launch_pspmv<T, false>(ctx, A->sell, Vals<T>::val(A->sell), z, p, p_next, q, state_beta(st));
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   return MTLGPU_OK;
 }
+
+// BiCGSTAB: s = r - alpha v with ||s|| and the half-step test in the first
+// L pass of shat = solve(M, s); the later passes skip on skip2.
+template <typename T>
+mtlgpu_status bicg_fused_s_apply(Csr* A, Pc* P, SolverState* st, const T* r, const T* v, T* s,
+                                 T* shat) {
+  return fused_apply<T, true>(A->ctx, P, st, nullptr, nullptr, r, v, s, shat, &st->skip2,
+                              nullptr, nullptr);
+}
+
+template mtlgpu_status bicg_fused_s_apply<double>(Csr*, Pc*, SolverState*, const double*,
+                                                  const double*, double*, double*);
+template mtlgpu_status bicg_fused_s_apply<float>(Csr*, Pc*, SolverState*, const float*,
+                                                 const float*, float*, float*);
 
 template <typename T>
 mtlgpu_status bicg_t_product(Csr* A, SolverState* st, const T* shat, const T* s, T* t) {

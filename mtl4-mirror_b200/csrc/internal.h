@@ -304,6 +304,9 @@ bool cg_fused_eligible(Csr* A, Pc* P, int prec);
 template <typename T>
 mtlgpu_status cg_fused_prologue(Csr* A, Pc* P, SolverState* st, const T* r, T* z, T* p, T* q);
 template <typename T>
+mtlgpu_status bicg_fused_s_apply(Csr* A, Pc* P, SolverState* st, const T* r, const T* v, T* s,
+                                 T* shat);
+template <typename T>
 mtlgpu_status bicg_t_product(Csr* A, SolverState* st, const T* shat, const T* s, T* t);
 template <typename T>
 mtlgpu_status cg_direction_product(Csr* A, const T* z, double beta, const T* p, T* p_next, T* q,

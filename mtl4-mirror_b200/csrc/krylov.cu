@@ -599,11 +599,18 @@ mtlgpu_status record_bicgstab_iteration(Workspace<T>* W) {
   a.out = &W->st->gamma;
   a.skip = &W->st->done;
   MTLGPU_TRY(spmv_launch<T>(A, W->phat, W->v, a));
-  bicg_s_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->v, W->s, sw ? tmp : nullptr,
-                                                     sw ? W->shat : nullptr, W->st,
-                                                     ctx->d_partials, counter_slot(ctx, 4));
-  // shat = solve(M, s); t = A shat; omega
-  MTLGPU_TRY(apply_pc<T>(W, W->s, W->shat, &W->st->skip2, sw));
+  if (W->fused) {
+    // s = r - alpha v, ||s|| and the half-step test in the first L pass of
+    // shat = solve(M, s)
+    MTLGPU_TRY(bicg_fused_s_apply<T>(A, W->P, W->st, W->r, W->v, W->s, W->shat));
+  } else {
+    bicg_s_kernel<T><<<grid, kBlock, 0, ctx->stream>>>(n, W->r, W->v, W->s, sw ? tmp : nullptr,
+                                                       sw ? W->shat : nullptr, W->st,
+                                                       ctx->d_partials, counter_slot(ctx, 4));
+    // shat = solve(M, s)
+    MTLGPU_TRY(apply_pc<T>(W, W->s, W->shat, &W->st->skip2, sw));
+  }
+  // t = A shat; omega
   if (W->fused) {
     MTLGPU_TRY(bicg_t_product<T>(A, W->st, W->shat, W->s, W->t));  // t and omega's dots
   } else {
