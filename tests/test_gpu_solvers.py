@@ -223,3 +223,38 @@ def test_config2_full_pcg_fp64_and_mixed(M, ctx, golden):
     dx.upload(np.zeros(A[0]))
     st, res, _ = M.solve("cg", dA, P32, dx, db, rtol=1e-10, max_iter=4000, mode=M.SOLVE_MIXED)
     assert st == M.OK and true_rel(M, A, dx.download(), b) <= 1e-10
+
+
+@pytest.mark.parametrize("method,pc,A_fn,kw", [
+    ("cg", "ic0", lambda M: M.laplacian3d(20), {}),
+    ("bicgstab", "ilu0", lambda M: M.convdiff27(12, 2), {}),
+    ("cg", "ic0", lambda M: M.laplacian3d(24), {"jacobi": 1}),
+    ("cg", "identity", lambda M: M.laplacian2d(40, 40), {"max_iter": 37}),
+])
+def test_device_loop_matches_host_loop(M, ctx, method, pc, A_fn, kw):
+    # Without an interrupt flag the iterations repeat in a device-side graph
+    # loop; with one (held at 0) the host relaunches the graph and polls the
+    # flag between launches.  Both run the same recorded kernels in the same
+    # order: the same iterations, residual history and solution, bit for bit,
+    # including a solve stopped by its iteration limit in mid-graph.
+    A = A_fn(M)
+    n = A[0]
+    b = M.csr_mult(A, M.uniform(n, 1))
+    dA = M.Csr(ctx, *A[1:])
+    P = None if pc == "identity" else M.Pc(dA, pc)
+    if kw.get("jacobi"):
+        P.set_jacobi_sweeps(kw["jacobi"])
+    max_iter = kw.get("max_iter", 2000)
+    out = []
+    for flag in (None, np.zeros(1, np.int32)):
+        dx, db = ctx.to_device(np.zeros(n)), ctx.to_device(b)
+        st, res, hist = M.solve(method, dA, P, dx, db, rtol=1e-10, max_iter=max_iter,
+                                interrupt=flag)
+        out.append((st, res.iterations, np.array(hist), dx.download()))
+    (s0, i0, h0, x0), (s1, i1, h1, x1) = out
+    assert s0 == s1 and i0 == i1
+    assert np.array_equal(h0, h1) and np.array_equal(x0, x1)
+    if "max_iter" in kw:
+        assert s0 == M.MAX_ITER and i0 == max_iter
+    else:
+        assert s0 == M.OK
