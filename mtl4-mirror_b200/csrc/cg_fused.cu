@@ -23,6 +23,13 @@
 // p, z each read once less, two launches and one grid reduction fewer).
 // The first iteration's front half (z, rho, p = z, q, alpha_1) is a
 // prologue run once before the graph.
+//
+// itl::bicgstab (itl/krylov/bicgstab.hpp:27-78) with Jacobi-applied factors
+// takes two pieces from here: K_A in its BiCGSTAB form (s = r - alpha v,
+// ||s|| and the half-step test, fused into the first L pass of
+// shat = solve(M, s)) and bicg_tprod_kernel (t = A shat with omega's dots
+// t.s and t.t).  The product kernel K_C is also the C-ABI operation
+// mtlgpu_cg_direction_product.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
