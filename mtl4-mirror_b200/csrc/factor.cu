@@ -205,15 +205,26 @@ __device__ __forceinline__ int find_col(const int32_t* __restrict__ ci, int b, i
   return -1;
 }
 
+// Pivot rows of at most this many entries are searched in shared memory.
+constexpr int kIluRowCache = 64;
+
 // ILU(0), one warp per row, rows in level order of the strict-lower pattern.
-// lu holds A's values in A's CSR layout and is updated in place.
+// lu holds A's values in A's CSR layout and is updated in place.  For each
+// pivot row k of row i the warp loads row k's columns and (final) values
+// into its shared buffer with one coalesced pass, and every lane finds its
+// column there by binary search: one global round trip per pivot instead of
+// a chain of dependent global loads per lane.  The arithmetic and its order
+// are unchanged (longer pivot rows are searched in global memory).
 __global__ void __launch_bounds__(kBlock)
     ilu0_kernel(int n_tasks, const int32_t* __restrict__ task_ptr,
                 const int32_t* __restrict__ row_of, const int32_t* __restrict__ rp,
                 const int32_t* __restrict__ ci, const int32_t* __restrict__ diag, double* lu,
                 double* inv_dia, int* done, unsigned* ticket, int* err, int* pivot,
                 long long limit) {
+  __shared__ int32_t row_col[kBlock / 32][kIluRowCache];
+  __shared__ double row_val[kBlock / 32][kIluRowCache];
   const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
   while (true) {
     unsigned t = 0;
     if (lane == 0) t = atomicAdd(ticket, 1u);
@@ -222,6 +233,60 @@ __global__ void __launch_bounds__(kBlock)
     for (int p = task_ptr[t]; p < task_ptr[t + 1]; p++) {
       const int i = row_of[p];
       const int b = rp[i], e = rp[i + 1];
+      if (e - b <= 32) {
+        // the row in registers (lane q holds entry b + q) for the whole
+        // elimination; the same operations in the same order as below
+        const int len = e - b;
+        const int mycol = lane < len ? __ldg(ci + b + lane) : 0x7fffffff;
+        double my = lane < len ? lu[b + lane] : 0.0;
+        for (int kq = 0; kq < len; kq++) {
+          const int k = __shfl_sync(0xffffffffu, mycol, kq);
+          if (k == i) break;
+          if (lane == 0) {
+            long long spins = 0;
+            while (ld_acquire(done + k) == 0) {
+              if (++spins >= limit) {
+                atomicCAS(err, 0, (int)MTLGPU_TIMEOUT);
+                break;
+              }
+              if ((spins & 1023) == 0 && ld_relaxed(err) != 0) break;
+            }
+          }
+          __syncwarp();
+          const double aik = __dmul_rn(__shfl_sync(0xffffffffu, my, kq), __ldcg(inv_dia + k));
+          if (lane == kq) my = aik;
+          const int kb = rp[k], ke = rp[k + 1];
+          const bool upd = lane > kq && lane < len;
+          if (ke - kb <= kIluRowCache) {
+            for (int q = lane; q < ke - kb; q += 32) {
+              row_col[wid][q] = __ldg(ci + kb + q);
+              row_val[wid][q] = __ldcg(lu + kb + q);
+            }
+            __syncwarp();
+            if (upd) {
+              const int pos = find_col(row_col[wid], 0, ke - kb, mycol);
+              my = __dsub_rn(my, __dmul_rn(aik, pos >= 0 ? row_val[wid][pos] : 0.0));
+            }
+          } else if (upd) {
+            const int pos = find_col(ci, kb, ke, mycol);
+            my = __dsub_rn(my, __dmul_rn(aik, pos >= 0 ? __ldcg(lu + pos) : 0.0));
+          }
+          __syncwarp();
+        }
+        if (lane < len) lu[b + lane] = my;
+        const int d = diag[i];
+        const double dv = __shfl_sync(0xffffffffu, my, d >= b && d < e ? d - b : 0);
+        __syncwarp();
+        if (lane == 0) {
+          const double piv = d >= 0 ? dv : 0.0;
+          if (bad_pivot(piv)) atomicCAS(pivot, 0, (int)MTLGPU_ZERO_PIVOT);
+          inv_dia[i] = __ddiv_rn(1.0, piv);
+          __threadfence();
+          st_release(done + i, 1);
+        }
+        __syncwarp();
+        continue;
+      }
       for (int kc = b; kc < e; kc++) {
         const int k = ci[kc];
         if (k == i) break;
@@ -241,10 +306,23 @@ __global__ void __launch_bounds__(kBlock)
         __syncwarp();
         if (lane == 0) lu[kc] = aik;
         const int kb = rp[k], ke = rp[k + 1];
-        for (int jc = kc + 1 + lane; jc < e; jc += 32) {
-          const int pos = find_col(ci, kb, ke, ci[jc]);
-          const double ukj = pos >= 0 ? __ldcg(lu + pos) : 0.0;
-          lu[jc] = __dsub_rn(lu[jc], __dmul_rn(aik, ukj));
+        if (ke - kb <= kIluRowCache) {
+          for (int q = lane; q < ke - kb; q += 32) {
+            row_col[wid][q] = __ldg(ci + kb + q);
+            row_val[wid][q] = __ldcg(lu + kb + q);
+          }
+          __syncwarp();
+          for (int jc = kc + 1 + lane; jc < e; jc += 32) {
+            const int pos = find_col(row_col[wid], 0, ke - kb, ci[jc]);
+            const double ukj = pos >= 0 ? row_val[wid][pos] : 0.0;
+            lu[jc] = __dsub_rn(lu[jc], __dmul_rn(aik, ukj));
+          }
+        } else {
+          for (int jc = kc + 1 + lane; jc < e; jc += 32) {
+            const int pos = find_col(ci, kb, ke, ci[jc]);
+            const double ukj = pos >= 0 ? __ldcg(lu + pos) : 0.0;
+            lu[jc] = __dsub_rn(lu[jc], __dmul_rn(aik, ukj));
+          }
         }
         __syncwarp();
       }
