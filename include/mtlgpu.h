@@ -132,7 +132,11 @@ typedef struct {
   const volatile int* h_interrupt; /* host flag (pinned or mapped memory is
                                       best); nonzero stops the solve with
                                       MTLGPU_INTERRUPTED between iterations,
-                                      as itl::interruptible_iteration */
+                                      as itl::interruptible_iteration.  The
+                                      flag is read between launches of 16
+                                      recorded iterations; a solve without
+                                      one repeats them in a device-side loop
+                                      (one launch, no host round trips) */
 } mtlgpu_iter_params;
 
 typedef struct {
