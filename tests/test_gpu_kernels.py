@@ -387,3 +387,26 @@ def test_cg_direction_product(M, ctx, restate, A_fn):
     assert rel_err(q, q64) <= 1e-6
     assert abs(pq - np.dot(po, q)) <= 1e-6 * abs(np.dot(po, q))
     dA.close()
+
+
+@pytest.mark.parametrize("kind", ["ic0", "ilu0"])
+def test_factors_bit_exact_full_size(M, ctx, restate, kind):
+    # The configurations' own factorisations: IC(0) of the 128^3 7-point
+    # Laplacian (n = 2,097,152) and ILU(0) of the 96^3 27-point
+    # convection-diffusion operator (n = 884,736, seed 2), bit-identical to
+    # the C restatement of the reference's factorisations, with the same
+    # level arrays (the level analysis takes rows in chunks, and ILU(0)
+    # keeps short rows in registers: both must leave the results unchanged).
+    A = M.laplacian3d(128) if kind == "ic0" else M.convdiff27(96, 2)
+    dA = M.Csr(ctx, *A[1:])
+    P = M.Pc(dA, kind)
+    L, U = getattr(restate, kind)(A)
+    assert csr_eq(P.factor(M.LOWER), L), "L pattern/values differ"
+    assert csr_eq(P.factor(M.UPPER), U), "U pattern/values differ"
+    lv, nl = restate.levels(L, True)
+    uv, nu = restate.levels(U, False)
+    assert np.array_equal(P.levels(M.LOWER), lv)
+    assert np.array_equal(P.levels(M.UPPER), uv)
+    assert P.factor_info(M.LOWER)[1] == nl and P.factor_info(M.UPPER)[1] == nu
+    P.close()
+    dA.close()
