@@ -258,3 +258,36 @@ def test_device_loop_matches_host_loop(M, ctx, method, pc, A_fn, kw):
         assert s0 == M.MAX_ITER and i0 == max_iter
     else:
         assert s0 == M.OK
+
+
+@pytest.mark.parametrize("method,pc", [("cg", "ic0"), ("bicgstab", "ilu0"), ("cg", None)])
+@pytest.mark.parametrize("mixed", [False, True])
+@pytest.mark.parametrize("jacobi", [0, 1])
+def test_empty_and_one_row_systems(M, ctx, method, pc, mixed, jacobi):
+    # n = 0: ||b|| = 0, so basic_iteration converges before the first
+    # iteration (basic_iteration.hpp:85-93), as the reference's solvers do on
+    # an empty system.  n = 1: the 1 x 1 system 4 x = 8.
+    if pc is None and jacobi:
+        pytest.skip("Jacobi iterations apply factors")
+    kw = dict(mode=M.SOLVE_MIXED, inner_rtol=1e-5) if mixed else {}
+    prec = M.FP32 if mixed else M.FP64
+    dA = M.Csr(ctx, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    P = M.Pc(dA, pc, prec) if pc else None
+    if P and jacobi:
+        P.set_jacobi_sweeps(jacobi)
+    dx, db = ctx.array(0), ctx.array(0)
+    st, res, _ = M.solve(method, dA, P, dx, db, rtol=1e-10, max_iter=10, **kw)
+    assert st == M.OK and res.iterations == 0
+    if P:
+        P.close()
+    dA.close()
+    dA = M.Csr(ctx, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([4.0]))
+    P = M.Pc(dA, pc, prec) if pc else None
+    if P and jacobi:
+        P.set_jacobi_sweeps(jacobi)
+    dx, db = ctx.to_device(np.zeros(1)), ctx.to_device(np.array([8.0]))
+    st, res, _ = M.solve(method, dA, P, dx, db, rtol=1e-10, max_iter=10, **kw)
+    assert st == M.OK and abs(dx.download()[0] - 2.0) <= 1e-12
+    if P:
+        P.close()
+    dA.close()
