@@ -119,3 +119,21 @@ def test_batched_sharded_two_gloo_ranks(tmp_path):
     assert o["ranks"] == 2 and o["all_systems_once"] and sum(o["per_rank_systems"]) == 512
     assert o["ms"] == max(o["per_rank_ms"])
     assert max(o["per_rank_ms"]) <= 1.01 * min(o["per_rank_ms"])
+
+
+def test_sell_index_bytes_follows_the_library_rule(M, monkeypatch):
+    # The bench counts 2 bytes of column index per entry where the library's
+    # SELL-32 copies hold 16-bit offsets (every entry within 32,767 of its
+    # row, MTLGPU_SELL_INDEX not 32), else 4.
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    n, rp, ci, v = M.laplacian3d(16)
+    assert bench.sell_index_bytes(rp, ci) == 2
+    rp2 = np.array([0, 2, 3], np.int32)
+    assert bench.sell_index_bytes(rp2, np.array([0, 1, 1], np.int32)) == 2
+    far_rp = np.array([0, 1] + [1] * 32767 + [2], np.int32)  # 32,769 rows
+    assert bench.sell_index_bytes(far_rp, np.array([32767, 0], np.int32)) == 2
+    assert bench.sell_index_bytes(far_rp, np.array([32768, 0], np.int32)) == 4
+    monkeypatch.setenv("MTLGPU_SELL_INDEX", "32")
+    assert bench.sell_index_bytes(rp, ci) == 4
