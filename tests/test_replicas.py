@@ -132,8 +132,9 @@ def test_sell_index_bytes_follows_the_library_rule(M, monkeypatch):
     assert bench.sell_index_bytes(rp, ci) == 2
     rp2 = np.array([0, 2, 3], np.int32)
     assert bench.sell_index_bytes(rp2, np.array([0, 1, 1], np.int32)) == 2
-    far_rp = np.array([0, 1] + [1] * 32767 + [2], np.int32)  # 32,769 rows
-    assert bench.sell_index_bytes(far_rp, np.array([32767, 0], np.int32)) == 2
-    assert bench.sell_index_bytes(far_rp, np.array([32768, 0], np.int32)) == 4
+    # 32,769 rows: one entry in row 0, one in row 32,768 on its own column
+    far_rp = np.array([0, 1] + [1] * 32767 + [2], np.int32)
+    assert bench.sell_index_bytes(far_rp, np.array([32767, 32768], np.int32)) == 2
+    assert bench.sell_index_bytes(far_rp, np.array([32768, 32768], np.int32)) == 4
     monkeypatch.setenv("MTLGPU_SELL_INDEX", "32")
     assert bench.sell_index_bytes(rp, ci) == 4
