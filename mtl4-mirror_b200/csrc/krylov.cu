@@ -499,6 +499,7 @@ struct Workspace {
   size_t graph_nodes = 0;      // kernel nodes per graph launch
   cudaGraphExec_t exec_loop = nullptr;  // the same iterations in a device-side loop
   bool loop_failed = false;             // the loop graph could not be made: host loop
+  bool state_on_host = false;           // h_st already holds the finished solve's state
   ~Workspace() {}
 };
 
@@ -836,7 +837,11 @@ mtlgpu_status run_iterations(Workspace<T>* W, const volatile int* h_interrupt, i
                                          ctx->stream));
     MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->launches += (long long)W->h_st->trips * (long long)(W->graph_nodes + 1);
-    if (err || W->h_st->done) return take_device_error(ctx);
+    if (err) return take_device_error(ctx);
+    if (W->h_st->done) {
+      W->state_on_host = true;  // h_st is the final state; the error word is clear
+      return MTLGPU_OK;
+    }
     // the trip bound ended the loop first: the host loop below carries on
   }
   while (true) {
@@ -940,11 +945,14 @@ mtlgpu_status device_solve(Workspace<T>* W, const mtlgpu_iter_params* prm, doubl
   }
   MTLGPU_TRY_CUDA(ctx, cudaGetLastError());
   int interrupted = 0;
+  W->state_on_host = false;
   MTLGPU_TRY(run_iterations<T>(W, prm->h_interrupt, &interrupted));
   SolverState* h = W->h_st;
-  MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h, W->st, sizeof(SolverState), cudaMemcpyDeviceToHost,
-                                       ctx->stream));
-  MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!W->state_on_host) {
+    MTLGPU_TRY_CUDA(ctx, cudaMemcpyAsync(h, W->st, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    MTLGPU_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   *iters = h->iter;
   *err_code = h->error;
   *status = interrupted ? MTLGPU_INTERRUPTED : (h->status ? h->status : (h->error ? MTLGPU_MAX_ITER : MTLGPU_OK));
